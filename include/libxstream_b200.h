@@ -1,0 +1,79 @@
+/*
+ * Extension entry points of the B200 SMM library: additions beside the DBCSR ABI, for tuning,
+ * measurement and batched execution. None of them changes what libsmm_acc_process computes.
+ * Each declaration names the part of the reference it corresponds to, or says that it has none.
+ */
+#ifndef LIBXSTREAM_B200_H
+#define LIBXSTREAM_B200_H
+
+#include "libsmm_acc.h"
+
+#if defined(__cplusplus)
+extern "C" {
+#endif
+
+/** The suitability rule of libsmm_acc_process: 1 if the stack is handled on the GPU, else 0.
+    Replaces libsmm_acc_process_suitable (samples/smm/smm_acc.c:527-573). */
+int libxstream_b200_process_suitable(
+  c_dbcsr_acc_bool_t def_mnk, libsmm_acc_data_t datatype, int stack_size, int m, int n, int k, int max_kernel_dim);
+
+/** Last CUDA error code recorded by the library (0 if none); cleared by c_dbcsr_acc_clear_errors.
+    Corresponds to the reference's error slot (libxstream/libxstream_opencl.h:156-194). */
+int libxstream_b200_last_error(void);
+
+/** FP64 tensor-pipe (DMMA) peak of the active device in TFLOP/s, measured by a short kernel on
+    the given stream (NULL: per-thread default stream). No counterpart in the reference. */
+double libxstream_b200_fp64_peak(void* stream);
+
+/** Set the kernel parameters used for FP64 stacks of shape (m, n, k): chunk = entries per warp
+    (0: size to each stack), mt/nt = warp sub-tile in 8x8 DMMA tiles (1..4), kp = k-steps per
+    register panel (2 or 4), wpb = warps per CTA (1..4). Replaces the OPENCL_LIBSMM_SMM_* tunables
+    (samples/smm/smm_kernel.c:194-278). Returns 0 on success. */
+int libxstream_b200_set_params(int m, int n, int k, int chunk, int mt, int nt, int kp, int wpb);
+
+/** Read back the parameters used for (m, n, k, stack_size): out6 = {chunk, mt, nt, kp, wpb, sorted}. */
+int libxstream_b200_get_params(int m, int n, int k, int stack_size, int* out6);
+
+/** Forget all tuned parameters (defaults apply afterwards). */
+void libxstream_b200_clear_params(void);
+
+/** Load tuned parameters from a CSV file (DEVICE;TYPEID;M;N;K;S;GFLOPS;L;MT;NT;KP;WPB), as the
+    reference loads OPENCL_LIBSMM_SMM_PARAMS (samples/smm/smm_acc.c:92-152). Returns the number of
+    records, or -1 if the file cannot be read. */
+int libxstream_b200_load_params(const char* csv_path);
+
+/** Test hook: the nth following device scratch allocation fails (0 disables). No counterpart in
+    the reference; used to check that allocation failures surface as nonzero return codes. */
+void libxstream_b200_inject_alloc_failure(int nth);
+
+/** Launch profile: when enabled (also by LIBXSTREAM_B200_PROFILE=1), each kernel launch is timed
+    with events on its stream and filed under its kernel name with the work it states (flops,
+    bytes). Counterpart of the reference's LIBXSTREAM_PROFILE per-kernel histogram
+    (src/libxstream.c:2629-2723). */
+void libxstream_b200_profile_enable(int on);
+void libxstream_b200_profile_reset(void);
+/** Totals for one kernel name; waits for its pending launches. Returns 0, or -1 if never launched. */
+int libxstream_b200_profile_query(const char* kernel, long* launches, double* ms, double* gflop, double* gbyte);
+/** Names of the profiled kernels, ';'-separated, into names[capacity]; returns the length used. */
+int libxstream_b200_profile_kernels(char* names, int capacity);
+
+/** A timing-enabled event (c_dbcsr_acc_event_create makes events without timing) and the time in
+    ms between two recorded ones (waits for `stop`; -1 on error). No counterpart in the reference. */
+int libxstream_b200_event_create_timed(void** event_p);
+double libxstream_b200_event_elapsed_ms(void* start, void* stop);
+
+/** CUDA-graph capture of library calls: begin capturing the calls made on `stream` by this thread,
+    end the capture into an executable graph (nkernels, if given, receives its number of kernel
+    nodes), replay it on a stream, destroy it. A captured libsmm_acc_process replays with the
+    arguments and buffers it was captured with. No counterpart in the reference (it enqueues every
+    kernel individually, samples/smm/smm_kernel.c:462-507). */
+int libxstream_b200_graph_begin(void* stream);
+int libxstream_b200_graph_end(void* stream, void** graph_exec, int* nkernels);
+int libxstream_b200_graph_launch(void* graph_exec, void* stream);
+int libxstream_b200_graph_destroy(void* graph_exec);
+
+#if defined(__cplusplus)
+}
+#endif
+
+#endif /* LIBXSTREAM_B200_H */

@@ -1,0 +1,106 @@
+/*
+ * Internal declarations shared by the C host layer (acc_runtime.c, smm_acc.c, smm_params.c) and
+ * the CUDA translation units (smm_kernels.cu and friends). Nothing here is part of the public ABI.
+ */
+#ifndef LIBXSTREAM_B200_INTERNAL_H
+#define LIBXSTREAM_B200_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__cplusplus)
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- runtime state (acc_runtime.c) */
+
+/** Make sure the calling thread has the active device current; returns 0 on success. */
+int xs_ensure_device(void);
+/** Active device id (set by c_dbcsr_acc_set_active_device, default 0). */
+int xs_active_device(void);
+/** Number of SMs of the active device (cached). */
+int xs_sm_count(void);
+/** Record a CUDA error code (nonzero) in the error slot; returns EXIT_FAILURE if code != 0. */
+int xs_record_error(int cuda_error, const char* where);
+/** Last recorded error code (0 if none). */
+int xs_last_error(void);
+/** Verbosity from LIBXSTREAM_B200_VERBOSE (0 = quiet). */
+int xs_verbosity(void);
+/** The stream used when the caller passes NULL: the per-thread default stream. */
+void* xs_default_stream(void);
+/** Stream-ordered scratch allocation from the device's memory pool (no host sync). */
+int xs_scratch_alloc(void** ptr, size_t nbytes, void* stream);
+int xs_scratch_free(void* ptr, void* stream);
+/** Test hook: make the n-th following scratch allocation fail (0 disables). */
+void xs_inject_alloc_failure(int nth);
+
+/* ------------------------------------------------------------------ launch profile (profile.c) */
+
+/** 1 if per-kernel launch profiling is on. */
+int xs_profile_enabled(void);
+/** Record a start event on the stream (NULL when profiling is off). */
+void* xs_profile_begin(void* stream);
+/** Record the stop event and file the launch under `name` with its stated work. */
+void xs_profile_end(void* token, const char* name, double flops, double bytes, void* stream);
+
+/* ------------------------------------------------ kernel launchers (smm_kernels.cu, C linkage) */
+
+/** Parameters of the plain FP64 stack kernel; chosen by the parameter table / autotuner. */
+typedef struct xs_smm_params_t {
+  int chunk;   /* entries per work item (L) */
+  int mt, nt;  /* warp sub-tile, in units of 8x8 DMMA tiles (1..4 each) */
+  int kp;      /* k-steps (of 4) per register panel: 2 or 4 */
+  int wpb;     /* warps per CTA */
+  int sorted;  /* 1: the stack is known to be grouped by c (skip the device sort) */
+} xs_smm_params_t;
+
+/** Size in bytes of the device scratch needed by xs_launch_smm_f64 for this call. */
+size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params);
+
+/**
+ * Plain FP64 stack multiply: sort by c (stable), chunked DMMA accumulation, single write-back per
+ * C block piece, deterministic combine of pieces. scratch must hold xs_smm_f64_scratch_bytes().
+ * Returns a cudaError_t value (0 = success).
+ */
+int xs_launch_smm_f64(const int* dev_stack, int stack_size, const double* a, const double* b, double* c, int m, int n,
+  int k, const xs_smm_params_t* params, void* scratch, size_t scratch_bytes, void* stream);
+
+/** Stable grouping of a stack by c (stack_sort.cu): extract splits the AoS stack into keys (c) and
+    payload (a | b << 32), resets the segment list and gathers the bucket statistics; sort writes
+    the grouped order to (kout, vout) using (k0, v0) and (k1, v1) as ping-pong buffers. */
+size_t xs_stack_sort_scratch_bytes(int S);
+int xs_stack_extract(const int* dev_stack, int S, unsigned* keys, unsigned long long* vals, int* seglist, void* sort_scratch,
+  void* stream);
+int xs_stack_sort(int S, unsigned* k0, unsigned long long* v0, unsigned* k1, unsigned long long* v1, unsigned* kout,
+  unsigned long long* vout, void* sort_scratch, void* stream);
+/** Reads the sort's error flag (1 = a grid barrier timed out); synchronises the stream. */
+int xs_stack_sort_error(void* sort_scratch, int* err, void* stream);
+
+/** In-place batched transpose of m x n blocks (element size esize: 4 or 8). Returns cudaError_t. */
+int xs_launch_transpose(const int* dev_trs_stack, int offset, int stack_size, void* data, int esize, int m, int n,
+  void* stream);
+
+/** Block Frobenius norms (c_calculate_norms). Returns cudaError_t. */
+int xs_launch_norms(const double* mat, int nblks, const int* offsets, const int* nelems, float* norms, void* stream);
+
+/** Measured FP64 DMMA peak (TFLOP/s) via a short microbenchmark on the active device. */
+double xs_fp64_peak_tflops(void* stream);
+
+/* ------------------------------------------------------------- parameter table (smm_params.c) */
+
+/** Look up tuned parameters for (type, m, n, k); fills defaults if none are known. */
+void xs_params_lookup(int type, int m, int n, int k, int stack_size, xs_smm_params_t* out);
+/** Default heuristic parameters (used when the table has no entry). */
+void xs_params_default(int m, int n, int k, int stack_size, xs_smm_params_t* out);
+/** Load a CSV parameter table (returns number of records or -1). */
+int xs_params_load_csv(const char* path);
+/** Drop all table entries. */
+void xs_params_clear(void);
+/** Insert/replace one record. */
+int xs_params_set(int type, int m, int n, int k, const xs_smm_params_t* p, double gflops);
+
+#if defined(__cplusplus)
+}
+#endif
+
+#endif /* LIBXSTREAM_B200_INTERNAL_H */

@@ -1,0 +1,600 @@
+/*
+ * sm_100a kernels for the DBCSR stack path: plain FP64 stack multiply, batched in-place transpose,
+ * block norms, and the FP64 tensor-pipe peak probe.
+ *
+ * Plain FP64 stack multiply (replaces samples/smm/kernels/multiply.cl:80-701 and the launch in
+ * samples/smm/smm_kernel.c:462-507). Semantics per stack entry (a, b, c), 1-based offsets:
+ *     C(i,j) += sum_kk A(i,kk) * B(kk,j),   A(i,kk) = a[a-1 + kk*m + i]   (m x k, column-major)
+ *                                           B(kk,j) = b[b-1 + kk*n + j]   (pre-transposed k x n)
+ *                                           C(i,j)  = c[c-1 + j*m + i]    (m x n, column-major)
+ * (multiply.cl:12-15 ADX/BDX/CDX with IDX/IDT from libxstream_common.h:86-87).
+ *
+ * B200 design, instead of the reference's one-work-group-per-mini-batch with FP atomics at every
+ * change of c (multiply.cl:621-695):
+ *   1. The stack's c offsets are sorted stably (device radix sort): entries of one C block become
+ *      a contiguous segment, in stack order.
+ *   2. The sorted stack is cut into chunks of L entries (perfect load balance whatever the c
+ *      distribution). One warp owns one chunk and one warp sub-tile of C (8*MT x 8*NT). It streams
+ *      DMMA fragments (mma.sync m8n8k4 f64) straight from L2/HBM into registers, one k-panel ahead
+ *      of the tensor pipe, and keeps the C sub-tile in registers across the whole segment.
+ *   3. A segment that lies inside one chunk is written back once (red.global.add.f64: a single
+ *      writer per element, so the result is deterministic). A segment that crosses chunk
+ *      boundaries leaves one partial tile ("piece") per chunk in scratch; a second kernel sums the
+ *      pieces of each such segment in a fixed order and writes the block once.
+ *   The result is bitwise reproducible from run to run, unlike FP atomics.
+ */
+#include "internal.h"
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace {
+
+/* Warps of the combine kernel (its warp partials go through dynamic shared memory). */
+constexpr int kCombineWarps = 16;
+
+__device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+/* Per-lane geometry of a warp sub-tile: which rows/cols of C (and of the A/B fragments) it owns. */
+template <int MT, int NT>
+struct Tile {
+  int row[MT];  /* A row loaded for fragment tile i (g-th row of tile i) */
+  int col[NT];  /* B col loaded for fragment tile j */
+  bool rok[MT], cok[NT];
+  int r0, c0;
+  __device__ __forceinline__ void init(int sub, int nsub_n, int m, int n, int g) {
+    const int sm = sub / nsub_n, sn = sub - sm * nsub_n;
+    r0 = sm * 8 * MT;
+    c0 = sn * 8 * NT;
+#pragma unroll
+    for (int i = 0; i < MT; ++i) {
+      row[i] = r0 + 8 * i + g;
+      rok[i] = row[i] < m;
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      col[j] = c0 + 8 * j + g;
+      cok[j] = col[j] < n;
+    }
+  }
+};
+
+template <int MT, int NT, int KP>
+__device__ __forceinline__ void load_panel(double (&fa)[KP][MT], double (&fb)[KP][NT], const double* __restrict__ A,
+  const double* __restrict__ B, unsigned long long v, int ks0, int t, int m, int n, int k, const Tile<MT, NT>& tl) {
+  const size_t aoff = (size_t)((unsigned)v) - 1, boff = (size_t)((unsigned)(v >> 32)) - 1;
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    const int kk = 4 * (ks0 + p) + t;
+    const bool okk = kk < k;
+    const double* const ap = A + aoff + (size_t)kk * m;
+    const double* const bp = B + boff + (size_t)kk * n;
+#pragma unroll
+    for (int i = 0; i < MT; ++i) fa[p][i] = (okk && tl.rok[i]) ? __ldg(ap + tl.row[i]) : 0.0;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) fb[p][j] = (okk && tl.cok[j]) ? __ldg(bp + tl.col[j]) : 0.0;
+  }
+}
+
+template <int MT, int NT, int KP>
+__device__ __forceinline__ void mma_panel(double (&acc)[MT][NT][2], const double (&fa)[KP][MT], const double (&fb)[KP][NT],
+  int ks0, int KS) {
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    if (ks0 + p < KS) {
+#pragma unroll
+      for (int i = 0; i < MT; ++i) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], fa[p][i], fb[p][j]);
+      }
+    }
+  }
+}
+
+/* Write-back of a finished C sub-tile: each element has exactly one writer. */
+template <int MT, int NT>
+__device__ __forceinline__ void commit_tile(double* __restrict__ C, size_t coff, const double (&acc)[MT][NT][2], int m,
+  int n, int g, int t, const Tile<MT, NT>& tl) {
+#pragma unroll
+  for (int i = 0; i < MT; ++i) {
+    const int r = tl.r0 + 8 * i + g;
+    if (r < m) {
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int cc = tl.c0 + 8 * j + 2 * t;
+        if (cc < n) atomicAdd(C + coff + (size_t)cc * m + r, acc[i][j][0]);
+        if (cc + 1 < n) atomicAdd(C + coff + (size_t)(cc + 1) * m + r, acc[i][j][1]);
+      }
+    }
+  }
+}
+
+/* Shared memory of the stack kernel: per warp two partial tiles (head / tail piece) + metadata. */
+template <int MT, int NT>
+__host__ __device__ constexpr size_t smm_smem_bytes(int warps) {
+  return (size_t)warps * (2 * MT * NT * 2 * 32 * sizeof(double) + 4 * sizeof(int));
+}
+
+/* The stack kernel. CTA = W warps = W consecutive chunks of L sorted entries, one warp sub-tile.
+   Segments inside a chunk are written back directly. Pieces of segments that cross chunk
+   boundaries are merged inside the CTA through shared memory (in warp order); only segments that
+   cross the CTA's own boundaries leave a CTA-level piece in global scratch for the combine kernel. */
+template <int MT, int NT, int KP>
+__global__ void __launch_bounds__(128) xs_smm_dmma_kernel(const unsigned* __restrict__ keys,
+  const unsigned long long* __restrict__ vals, int S, const double* __restrict__ A, const double* __restrict__ B,
+  double* __restrict__ C, int m, int n, int k, int L, int nchunks, int nsub_n, int nsub, double* __restrict__ pieces,
+  int* __restrict__ seglist) {
+  constexpr int REGS = MT * NT * 2;
+  extern __shared__ double smem[];
+  const int W = blockDim.x >> 5;
+  double* const sp = smem;                                       /* [W][2][REGS][32] */
+  int* const meta = (int*)(smem + (size_t)W * 2 * REGS * 32);    /* [W][4]: head, head_spans, tail, spare */
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int group = blockIdx.x / nsub, sub = blockIdx.x - group * nsub;
+  const int chunk = group * W + warp;
+  const int KS = (k + 3) >> 2, npan = (KS + KP - 1) / KP;
+  Tile<MT, NT> tl;
+  tl.init(sub, nsub_n, m, n, g);
+  if (0 == lane) {
+    meta[warp * 4 + 0] = 0;
+    meta[warp * 4 + 1] = 0;
+    meta[warp * 4 + 2] = 0;
+  }
+  __syncwarp();
+  if (chunk < nchunks) {
+    const int p0 = chunk * L, p1 = min(p0 + L, S);
+    const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
+    const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
+
+    double acc[MT][NT][2];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    double fa0[KP][MT], fb0[KP][NT], fa1[KP][MT], fb1[KP][NT];
+    unsigned key_cur = keys[p0];
+    unsigned long long v_cur = vals[p0];
+    unsigned long long v_nxt = (p0 + 1 < p1) ? vals[p0 + 1] : 0ull;
+    unsigned key_nxt = (p0 + 1 < p1) ? keys[p0 + 1] : 0u;
+    int e = p0, pan = 0, segstart = p0;
+    load_panel<MT, NT, KP>(fa0, fb0, A, B, v_cur, 0, t, m, n, k, tl);
+
+    /* One step: prefetch the next panel into (fan, fbn), run the current one from (fac, fbc),
+       finish a segment when its last entry is done, advance. Returns false when the chunk is done. */
+    auto step = [&](double (&fac)[KP][MT], double (&fbc)[KP][NT], double (&fan)[KP][MT], double (&fbn)[KP][NT]) -> bool {
+      const bool last_pan = (pan + 1 == npan);
+      const int e2 = last_pan ? e + 1 : e;
+      const int pan2 = last_pan ? 0 : pan + 1;
+      if (e2 < p1) load_panel<MT, NT, KP>(fan, fbn, A, B, last_pan ? v_nxt : v_cur, pan2 * KP, t, m, n, k, tl);
+      mma_panel<MT, NT, KP>(acc, fac, fbc, pan * KP, KS);
+      if (last_pan) {
+        const bool seg_end = (e + 1 == p1) || (key_nxt != key_cur);
+        if (seg_end) {
+          const bool crossl = headcross && (segstart == p0);
+          const bool crossr = tailcross && (e + 1 == p1);
+          if (!crossl && !crossr) {
+            commit_tile<MT, NT>(C, (size_t)key_cur - 1, acc, m, n, g, t, tl);
+          }
+          else { /* piece: head slot if it continues a segment from the previous chunk, else tail */
+            const int slot = crossl ? 0 : 1;
+            double* const dst = sp + ((size_t)(warp * 2 + slot) * REGS) * 32 + lane;
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+              for (int j = 0; j < NT; ++j) {
+                dst[((i * NT + j) * 2 + 0) * 32] = acc[i][j][0];
+                dst[((i * NT + j) * 2 + 1) * 32] = acc[i][j][1];
+              }
+            if (0 == lane) {
+              if (crossl) {
+                meta[warp * 4 + 0] = 1;
+                meta[warp * 4 + 1] = crossr ? 1 : 0;
+              }
+              else meta[warp * 4 + 2] = 1;
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+          segstart = e + 1;
+        }
+        if (e + 1 < p1) {
+          v_cur = v_nxt;
+          key_cur = key_nxt;
+          if (e + 2 < p1) {
+            v_nxt = vals[e + 2];
+            key_nxt = keys[e + 2];
+          }
+        }
+      }
+      e = e2;
+      pan = pan2;
+      return e < p1;
+    };
+    for (;;) {
+      if (!step(fa0, fb0, fa1, fb1)) break;
+      if (!step(fa1, fb1, fa0, fb0)) break;
+    }
+  }
+  __syncthreads();
+  /* CTA-level merge. Chains start at warp 0's head piece (a segment entering the CTA) and at every
+     tail piece (a segment starting in that warp's chunk); a chain continues through the head pieces
+     of the following warps while the previous piece reaches the end of its chunk. */
+  for (int start = 0; start < 2; ++start) {
+    const bool from_head = (0 == start);
+    if (from_head && 0 != warp) continue;
+    if (0 == meta[warp * 4 + (from_head ? 0 : 2)]) continue;
+    double sum[REGS];
+    const double* src = sp + ((size_t)(warp * 2 + (from_head ? 0 : 1)) * REGS) * 32 + lane;
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) sum[r] = src[r * 32];
+    bool spans = from_head ? (0 != meta[warp * 4 + 1]) : true;
+    int cur = warp;
+    while (spans && cur + 1 < W && group * W + cur + 1 < nchunks) {
+      ++cur;
+      src = sp + ((size_t)(cur * 2) * REGS) * 32 + lane;
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) sum[r] += src[r * 32];
+      spans = (0 != meta[cur * 4 + 1]);
+    }
+    const int c_first = group * W + warp; /* chunk where this chain starts */
+    if (from_head || spans) { /* the segment crosses a CTA boundary: CTA-level piece */
+      const int slot = from_head ? 2 * group : 2 * group + 1;
+      double* const dst = pieces + ((size_t)slot * nsub + sub) * REGS * 32 + lane;
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) dst[r * 32] = sum[r];
+      if (!from_head && 0 == sub && 0 == lane) {
+        const int slotidx = atomicAdd(seglist, 1);
+        seglist[1 + slotidx] = group;
+      }
+    }
+    else {
+      const int p1 = min((c_first + 1) * L, S);
+      const unsigned key = keys[p1 - 1]; /* a tail piece belongs to the last segment of its chunk */
+      double tile[MT][NT][2];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          tile[i][j][0] = sum[(i * NT + j) * 2 + 0];
+          tile[i][j][1] = sum[(i * NT + j) * 2 + 1];
+        }
+      commit_tile<MT, NT>(C, (size_t)key - 1, tile, m, n, g, t, tl);
+    }
+  }
+}
+
+/* Sum the pieces of every chunk-crossing segment in a fixed order and write the block once.
+   One CTA per (segment, sub-tile): its threads first find the segment's last chunk in one parallel
+   probe of chunk-start keys, then its warps sum the pieces round-robin (warp w takes pieces w,
+   w+CW, ...) and warp 0 adds the warp partials in warp order: the summation tree depends only on
+   the number of pieces, so the result is deterministic. */
+template <int MT, int NT>
+__global__ void __launch_bounds__(32 * kCombineWarps) xs_smm_combine_kernel(const unsigned* __restrict__ keys, int S,
+  int L, int nchunks, int nsub, int nsub_n, const double* __restrict__ pieces, const int* __restrict__ seglist,
+  double* __restrict__ C, int m, int n) {
+  constexpr int REGS = MT * NT * 2;
+  constexpr int CW = kCombineWarps;
+  extern __shared__ double red[]; /* [CW - 1][REGS][32] */
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int count = seglist[0];
+  for (int w = blockIdx.x; w < count * nsub; w += gridDim.x) {
+    const int li = w / nsub, sub = w - li * nsub;
+    const int j0 = seglist[1 + li];
+    const unsigned xkey = keys[min((j0 + 1) * L, S) - 1];
+    /* pieces = 1 + number of following chunks that start inside the segment (a prefix, keys sorted) */
+    int np = 1;
+    for (int base = j0 + 1;; base += blockDim.x) {
+      const int j = base + (int)threadIdx.x;
+      const int inside = (j < nchunks) && (keys[(size_t)j * L] == xkey);
+      const int cnt = __syncthreads_count(inside);
+      np += cnt;
+      if (cnt < (int)blockDim.x) break;
+    }
+    double acc[REGS];
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
+    int q = warp;
+    for (; q + CW < np; q += 2 * CW) { /* two pieces in flight per step */
+      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q), s1 = 2 * (j0 + q + CW);
+      const double* const p0 = pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
+      const double* const p1 = pieces + ((size_t)s1 * nsub + sub) * REGS * 32 + lane;
+      double v0[REGS], v1[REGS];
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) {
+        v0[r] = p0[r * 32];
+        v1[r] = p1[r * 32];
+      }
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += v0[r];
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += v1[r];
+    }
+    if (q < np) {
+      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q);
+      const double* const p0 = pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += p0[r * 32];
+    }
+    if (0 != warp) {
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) red[((warp - 1) * REGS + r) * 32 + lane] = acc[r];
+    }
+    __syncthreads();
+    if (0 == warp) {
+      for (int w2 = 0; w2 < CW - 1; ++w2) {
+#pragma unroll
+        for (int r = 0; r < REGS; ++r) acc[r] += red[(w2 * REGS + r) * 32 + lane];
+      }
+      Tile<MT, NT> tl;
+      tl.init(sub, nsub_n, m, n, g);
+      double tile[MT][NT][2];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          tile[i][j][0] = acc[(i * NT + j) * 2 + 0];
+          tile[i][j][1] = acc[(i * NT + j) * 2 + 1];
+        }
+      commit_tile<MT, NT>(C, (size_t)xkey - 1, tile, m, n, g, t, tl);
+    }
+    __syncthreads();
+  }
+}
+
+struct SmmPlan {
+  int nsub_m, nsub_n, nsub, nchunks, L, W, ngroups;
+  size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces;
+  size_t off_sort, total;
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl) {
+  (void)k;
+  const int mt = prm->mt, nt = prm->nt;
+  if (mt < 1 || mt > 4 || nt < 1 || nt > 4 || prm->chunk < 1) return -1;
+  pl->L = prm->chunk;
+  pl->nsub_m = ((m + 7) / 8 + mt - 1) / mt;
+  pl->nsub_n = ((n + 7) / 8 + nt - 1) / nt;
+  pl->nsub = pl->nsub_m * pl->nsub_n;
+  pl->nchunks = (S + pl->L - 1) / pl->L;
+  pl->W = (prm->wpb >= 1 && prm->wpb <= 4) ? prm->wpb : 4;
+  pl->ngroups = (pl->nchunks + pl->W - 1) / pl->W;
+  size_t off = 0;
+  const size_t ks = align_up(sizeof(unsigned) * (size_t)S, 256), vs = align_up(sizeof(unsigned long long) * (size_t)S, 256);
+  pl->off_keys_in = off;
+  off += ks;
+  pl->off_keys_tmp = off;
+  off += ks;
+  pl->off_keys_out = off;
+  off += ks;
+  pl->off_vals_in = off;
+  off += vs;
+  pl->off_vals_tmp = off;
+  off += vs;
+  pl->off_vals_out = off;
+  off += vs;
+  pl->off_seglist = off;
+  off = align_up(off + sizeof(int) * ((size_t)pl->nchunks + 1), 256);
+  pl->off_pieces = off;
+  off = align_up(off + sizeof(double) * (size_t)2 * pl->ngroups * pl->nsub * (mt * nt * 2) * 32, 256);
+  pl->off_sort = off;
+  off = align_up(off + xs_stack_sort_scratch_bytes(S), 256);
+  pl->total = off;
+  return 0;
+}
+
+template <int MT, int NT, int KP>
+cudaError_t launch_dmma(const SmmPlan& pl, const unsigned* keys, const unsigned long long* vals, int S, const double* a,
+  const double* b, double* c, int m, int n, int k, double* pieces, int* seglist, cudaStream_t s) {
+  cudaError_t r;
+  static int smem_set = 0, csmem_set = 0; /* per template instance; setting them twice is harmless */
+  const size_t smem = smm_smem_bytes<MT, NT>(pl.W);
+  if (smem > 48 * 1024 && smem_set < (int)smem) {
+    r = cudaFuncSetAttribute(xs_smm_dmma_kernel<MT, NT, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaSuccess != r) return r;
+    smem_set = (int)smem;
+  }
+  void* prof = xs_profile_begin(s);
+  xs_smm_dmma_kernel<MT, NT, KP><<<pl.ngroups * pl.nsub, 32 * pl.W, smem, s>>>(
+    keys, vals, S, a, b, c, m, n, k, pl.L, pl.nchunks, pl.nsub_n, pl.nsub, pieces, seglist);
+  r = cudaGetLastError();
+  if (cudaSuccess != r) return r;
+  xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)S, 8.0 * S * ((double)m * k + (double)k * n + 2.0 * m * n), s);
+  const int cgrid = max(1, min(pl.ngroups * pl.nsub, 2 * xs_sm_count()));
+  const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (MT * NT * 2) * 32;
+  if (!csmem_set) {
+    r = cudaFuncSetAttribute(xs_smm_combine_kernel<MT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+    if (cudaSuccess != r) return r;
+    csmem_set = 1;
+  }
+  prof = xs_profile_begin(s);
+  /* the combine works on CTA ranges: W*L entries per "chunk", one range per CTA group */
+  xs_smm_combine_kernel<MT, NT><<<cgrid, 32 * kCombineWarps, csmem, s>>>(
+    keys, S, pl.L * pl.W, pl.ngroups, pl.nsub, pl.nsub_n, pieces, seglist, c, m, n);
+  r = cudaGetLastError();
+  xs_profile_end(prof, "combine", 0.0, 0.0, s);
+  return r;
+}
+
+typedef cudaError_t (*launch_fn_t)(const SmmPlan&, const unsigned*, const unsigned long long*, int, const double*,
+  const double*, double*, int, int, int, double*, int*, cudaStream_t);
+
+#define XS_KP_ENTRY(MT, NT) {&launch_dmma<MT, NT, 2>, &launch_dmma<MT, NT, 4>}
+static const launch_fn_t launch_table[4][4][2] = {
+  {XS_KP_ENTRY(1, 1), XS_KP_ENTRY(1, 2), XS_KP_ENTRY(1, 3), XS_KP_ENTRY(1, 4)},
+  {XS_KP_ENTRY(2, 1), XS_KP_ENTRY(2, 2), XS_KP_ENTRY(2, 3), XS_KP_ENTRY(2, 4)},
+  {XS_KP_ENTRY(3, 1), XS_KP_ENTRY(3, 2), XS_KP_ENTRY(3, 3), XS_KP_ENTRY(3, 4)},
+  {XS_KP_ENTRY(4, 1), XS_KP_ENTRY(4, 2), XS_KP_ENTRY(4, 3), XS_KP_ENTRY(4, 4)},
+};
+
+/* ------------------------------------------------------------------------------ transpose */
+
+/* One CTA per block: stage the m x n column-major block in shared memory, write it back as n x m
+   column-major (transpose.cl:28-83 semantics; a bit copy, so exact for any element type). */
+template <typename T>
+__global__ void xs_transpose_kernel(const int* __restrict__ trs, int offset, int S, T* __restrict__ data, int m, int n) {
+  extern __shared__ unsigned char smem_raw[];
+  T* const buf = reinterpret_cast<T*>(smem_raw);
+  const int mn = m * n;
+  for (int blk = blockIdx.x; blk < S; blk += gridDim.x) {
+    T* const mat = data + trs[offset + blk];
+    for (int e = threadIdx.x; e < mn; e += blockDim.x) buf[e] = mat[e];
+    __syncthreads();
+    for (int o = threadIdx.x; o < mn; o += blockDim.x) {
+      const int i = o / n, j = o - i * n; /* output (j, i) of the n x m result = input (i, j) */
+      mat[o] = buf[j * m + i];
+    }
+    __syncthreads();
+  }
+}
+
+/* ---------------------------------------------------------------------------------- norms */
+
+__global__ void xs_norms_kernel(const double* __restrict__ mat, int nblks, const int* __restrict__ offsets,
+  const int* __restrict__ nelems, float* __restrict__ norms) {
+  const int lane = threadIdx.x & 31;
+  const int blk = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (blk >= nblks) return;
+  const double* const p = mat + offsets[blk];
+  const int ne = nelems[blk];
+  double s = 0.0;
+  for (int e = lane; e < ne; e += 32) s = fma(p[e], p[e], s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (0 == lane) norms[blk] = (float)sqrt(s);
+}
+
+/* ------------------------------------------------------------------------ FP64 peak probe */
+
+__global__ void xs_dmma_peak_kernel(double* out, int iters) {
+  const double a = 1.0 + threadIdx.x * 1e-6, b = 1.0 - threadIdx.x * 1e-6;
+  double c[8][2];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) c[u][0] = c[u][1] = 0.0;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) dmma_m8n8k4(c[u][0], c[u][1], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) s += c[u][0] + c[u][1];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params) {
+  SmmPlan pl;
+  if (0 >= stack_size || 0 != plan_smm(stack_size, m, n, k, params, &pl)) return 0;
+  return pl.total;
+}
+
+int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double* b, double* c, int m, int n, int k,
+  const xs_smm_params_t* prm, void* scratch, size_t scratch_bytes, void* stream) {
+  SmmPlan pl;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (0 >= S) return 0;
+  if (0 != plan_smm(S, m, n, k, prm, &pl) || scratch_bytes < pl.total || nullptr == scratch) return (int)cudaErrorInvalidValue;
+  char* const base = (char*)scratch;
+  unsigned* const keys_in = (unsigned*)(base + pl.off_keys_in);
+  unsigned* const keys_tmp = (unsigned*)(base + pl.off_keys_tmp);
+  unsigned* const keys_out = (unsigned*)(base + pl.off_keys_out);
+  unsigned long long* const vals_in = (unsigned long long*)(base + pl.off_vals_in);
+  unsigned long long* const vals_tmp = (unsigned long long*)(base + pl.off_vals_tmp);
+  unsigned long long* const vals_out = (unsigned long long*)(base + pl.off_vals_out);
+  int* const seglist = (int*)(base + pl.off_seglist);
+  double* const pieces = (double*)(base + pl.off_pieces);
+  void* const sort_scratch = base + pl.off_sort;
+  void* prof = xs_profile_begin(s);
+  int r = xs_stack_extract(dev_stack, S, keys_in, vals_in, seglist, sort_scratch, s);
+  if (0 != r) return r;
+  xs_profile_end(prof, "extract", 0.0, 24.0 * S, s);
+  const unsigned* keys = keys_in;
+  const unsigned long long* vals = vals_in;
+  if (!prm->sorted) {
+    prof = xs_profile_begin(s);
+    r = xs_stack_sort(S, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, sort_scratch, s);
+    if (0 != r) return r;
+    xs_profile_end(prof, "sort", 0.0, 24.0 * S, s);
+    keys = keys_out;
+    vals = vals_out;
+  }
+  const int kp = (4 == prm->kp) ? 1 : 0;
+  const launch_fn_t fn = launch_table[prm->mt - 1][prm->nt - 1][kp];
+  return (int)fn(pl, keys, vals, S, a, b, c, m, n, k, pieces, seglist, s);
+}
+
+int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize, int m, int n, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (0 >= S) return 0;
+  const int mn = m * n;
+  const size_t smem = (size_t)mn * esize;
+  int threads = ((mn + 31) / 32) * 32;
+  if (threads > 256) threads = 256;
+  const int grid = S < 64 * xs_sm_count() ? S : 64 * xs_sm_count();
+  cudaError_t r;
+  void* const prof = xs_profile_begin(s);
+  if (8 == esize) {
+    if (smem > 48 * 1024) {
+      r = cudaFuncSetAttribute(xs_transpose_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (cudaSuccess != r) return (int)r;
+    }
+    xs_transpose_kernel<unsigned long long><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned long long*)data, m, n);
+  }
+  else if (4 == esize) {
+    if (smem > 48 * 1024) {
+      r = cudaFuncSetAttribute(xs_transpose_kernel<unsigned>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (cudaSuccess != r) return (int)r;
+    }
+    xs_transpose_kernel<unsigned><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned*)data, m, n);
+  }
+  else return (int)cudaErrorInvalidValue;
+  r = cudaGetLastError();
+  xs_profile_end(prof, "trans", 0.0, 2.0 * esize * (double)mn * S, s);
+  return (int)r;
+}
+
+int xs_launch_norms(const double* mat, int nblks, const int* offsets, const int* nelems, float* norms, void* stream) {
+  if (0 >= nblks) return 0;
+  void* const prof = xs_profile_begin(stream);
+  xs_norms_kernel<<<(nblks + 7) / 8, 256, 0, (cudaStream_t)stream>>>(mat, nblks, offsets, nelems, norms);
+  const cudaError_t r = cudaGetLastError();
+  xs_profile_end(prof, "norms", 0.0, 0.0, stream);
+  return (int)r;
+}
+
+double xs_fp64_peak_tflops(void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const int sms = xs_sm_count(), threads = 256, blocks = sms * 8, iters = 4096;
+  double* out = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float ms = 0.f;
+  double result = -1.0;
+  if (cudaSuccess != cudaMallocAsync((void**)&out, sizeof(double) * blocks * threads, s)) return -1.0;
+  if (cudaSuccess == cudaEventCreate(&e0) && cudaSuccess == cudaEventCreate(&e1)) {
+    xs_dmma_peak_kernel<<<blocks, threads, 0, s>>>(out, 64); /* warm-up */
+    cudaEventRecord(e0, s);
+    xs_dmma_peak_kernel<<<blocks, threads, 0, s>>>(out, iters);
+    cudaEventRecord(e1, s);
+    if (cudaSuccess == cudaEventSynchronize(e1) && cudaSuccess == cudaEventElapsedTime(&ms, e0, e1) && 0 < ms) {
+      const double flops = 2.0 * 8 * 8 * 4 * 8 * (double)iters * blocks * (threads / 32);
+      result = flops / (ms * 1e-3) * 1e-12;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(out, s);
+  cudaStreamSynchronize(s);
+  return result;
+}
+
+}  // extern "C"

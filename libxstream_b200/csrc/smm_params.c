@@ -1,0 +1,165 @@
+/*
+ * Kernel-parameter table for the FP64 stack kernel: tuned records keyed by (type, m, n, k), read
+ * from and written to a semicolon-separated CSV whose leading columns are the reference's
+ * (DEVICE;TYPEID;M;N;K;S;GFLOPS, samples/smm/params/tune_multiply_*.csv line 1 and
+ * samples/smm/smm_params.c:89-270), followed by this library's tunables (L;MT;NT;KP;WPB).
+ * Replaces the reference's registry of JIT-ed kernels (samples/smm/smm_kernel.c:109-150): nothing
+ * is compiled at run time, a record only selects one of the precompiled kernel variants.
+ */
+#include "internal.h"
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define XS_PARAMS_CAP 8192 /* power of two */
+
+typedef struct xs_record_t {
+  int used, type, m, n, k;
+  double gflops;
+  xs_smm_params_t p;
+} xs_record_t;
+
+static xs_record_t xs_table[XS_PARAMS_CAP];
+static pthread_rwlock_t xs_table_lock = PTHREAD_RWLOCK_INITIALIZER;
+
+static unsigned xs_hash(int type, int m, int n, int k) {
+  unsigned h = 2166136261u;
+  h = (h ^ (unsigned)type) * 16777619u;
+  h = (h ^ (unsigned)m) * 16777619u;
+  h = (h ^ (unsigned)n) * 16777619u;
+  h = (h ^ (unsigned)k) * 16777619u;
+  return h;
+}
+
+static int xs_clamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+static void xs_sanitize(xs_smm_params_t* p) {
+  p->chunk = xs_clamp(p->chunk, 1, 4096);
+  p->mt = xs_clamp(p->mt, 1, 4);
+  p->nt = xs_clamp(p->nt, 1, 4);
+  p->kp = (4 == p->kp) ? 4 : 2;
+  p->wpb = xs_clamp(p->wpb, 1, 4);
+  p->sorted = (0 != p->sorted) ? 1 : 0;
+}
+
+/* Tiles of at most 4x4 DMMA fragments per warp; prefer the split of ceil(x/8) fragments into
+   equal sub-tiles with the least padding. */
+static int xs_pick_tiles(int dim) {
+  const int frags = (dim + 7) / 8;
+  int best = 1, bestwaste = 1 << 30, t;
+  for (t = 4; t >= 1; --t) {
+    const int nsub = (frags + t - 1) / t;
+    const int waste = nsub * t - frags;
+    if (waste < bestwaste) {
+      bestwaste = waste;
+      best = t;
+    }
+  }
+  return best;
+}
+
+void xs_params_default(int m, int n, int k, int stack_size, xs_smm_params_t* out) {
+  const int sms = xs_sm_count();
+  const int mt = xs_pick_tiles(m), nt = xs_pick_tiles(n);
+  const int nsub = ((((m + 7) / 8) + mt - 1) / mt) * ((((n + 7) / 8) + nt - 1) / nt);
+  /* about 16 resident warps per SM in one wave; never fewer than 4 entries per warp */
+  const long target_items = (long)sms * 16;
+  long chunk = ((long)stack_size * nsub + target_items - 1) / target_items;
+  (void)k;
+  if (chunk < 4) chunk = 4;
+  out->chunk = (int)chunk;
+  out->mt = mt;
+  out->nt = nt;
+  out->kp = ((k + 3) / 4 <= 2) ? 2 : 4;
+  out->wpb = 4;
+  out->sorted = 0;
+  xs_sanitize(out);
+}
+
+void xs_params_lookup(int type, int m, int n, int k, int stack_size, xs_smm_params_t* out) {
+  unsigned h = xs_hash(type, m, n, k) & (XS_PARAMS_CAP - 1);
+  int probe, found = 0;
+  pthread_rwlock_rdlock(&xs_table_lock);
+  for (probe = 0; probe < XS_PARAMS_CAP; ++probe) {
+    const xs_record_t* const r = &xs_table[(h + probe) & (XS_PARAMS_CAP - 1)];
+    if (!r->used) break;
+    if (r->type == type && r->m == m && r->n == n && r->k == k) {
+      *out = r->p;
+      found = 1;
+      break;
+    }
+  }
+  pthread_rwlock_unlock(&xs_table_lock);
+  if (!found) xs_params_default(m, n, k, stack_size, out);
+  else if (0 >= out->chunk) { /* a record may leave L open: size it to the stack */
+    xs_smm_params_t d;
+    xs_params_default(m, n, k, stack_size, &d);
+    out->chunk = d.chunk;
+  }
+}
+
+int xs_params_set(int type, int m, int n, int k, const xs_smm_params_t* p, double gflops) {
+  unsigned h = xs_hash(type, m, n, k) & (XS_PARAMS_CAP - 1);
+  int probe, result = -1;
+  pthread_rwlock_wrlock(&xs_table_lock);
+  for (probe = 0; probe < XS_PARAMS_CAP; ++probe) {
+    xs_record_t* const r = &xs_table[(h + probe) & (XS_PARAMS_CAP - 1)];
+    if (!r->used || (r->type == type && r->m == m && r->n == n && r->k == k)) {
+      if (!r->used || gflops >= r->gflops || 0 >= gflops) {
+        r->used = 1;
+        r->type = type;
+        r->m = m;
+        r->n = n;
+        r->k = k;
+        r->gflops = gflops;
+        r->p = *p;
+        xs_sanitize(&r->p);
+        if (0 >= p->chunk) r->p.chunk = 0; /* L left open: sized to each stack at lookup */
+      }
+      result = 0;
+      break;
+    }
+  }
+  pthread_rwlock_unlock(&xs_table_lock);
+  return result;
+}
+
+void xs_params_clear(void) {
+  pthread_rwlock_wrlock(&xs_table_lock);
+  memset(xs_table, 0, sizeof(xs_table));
+  pthread_rwlock_unlock(&xs_table_lock);
+}
+
+/* CSV: DEVICE;TYPEID;M;N;K;S;GFLOPS;L;MT;NT;KP;WPB (the first line is a header). */
+int xs_params_load_csv(const char* path) {
+  char line[1024];
+  int count = 0, lineno = 0;
+  FILE* const f = (NULL != path) ? fopen(path, "r") : NULL;
+  if (NULL == f) return -1;
+  while (NULL != fgets(line, sizeof(line), f)) {
+    char* fields[16];
+    int nf = 0;
+    char* tok = strtok(line, ";\n\r");
+    ++lineno;
+    while (NULL != tok && nf < 16) {
+      fields[nf++] = tok;
+      tok = strtok(NULL, ";\n\r");
+    }
+    if (1 == lineno && 0 < nf && NULL != strstr(fields[0], "DEVICE")) continue; /* header */
+    if (12 <= nf) {
+      xs_smm_params_t p;
+      const int type = atoi(fields[1]), m = atoi(fields[2]), n = atoi(fields[3]), k = atoi(fields[4]);
+      const double gflops = atof(fields[6]);
+      p.chunk = atoi(fields[7]);
+      p.mt = atoi(fields[8]);
+      p.nt = atoi(fields[9]);
+      p.kp = atoi(fields[10]);
+      p.wpb = atoi(fields[11]);
+      p.sorted = 0;
+      if (0 < m && 0 < n && 0 < k && 0 == xs_params_set(type, m, n, k, &p, gflops)) ++count;
+    }
+  }
+  fclose(f);
+  return count;
+}
