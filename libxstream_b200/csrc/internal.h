@@ -49,10 +49,15 @@ void xs_profile_end(void* token, const char* name, double flops, double bytes, v
 typedef struct xs_smm_params_t {
   int chunk;   /* entries per work item (L) */
   int mt, nt;  /* warp sub-tile, in units of 8x8 DMMA tiles (1..4 each) */
-  int kp;      /* k-steps (of 4) per register panel: 2 or 4 */
+  int kp;      /* k-steps (of 4) per register panel: 2 or 4 (1..4 for shape-specialised kernels) */
+  int generic; /* 1: always use the runtime-shape kernel even if a specialised one exists */
   int wpb;     /* warps per CTA */
   int sorted;  /* 1: the stack is known to be grouped by c (skip the device sort) */
 } xs_smm_params_t;
+
+/** Shape-specialised kernels compiled for (m, n, k): writes up to capacity (mt, nt, kp) triples,
+    returns how many exist. */
+int xs_smm_f64_specialized(int m, int n, int k, int* mt_nt_kp, int capacity);
 
 /** Size in bytes of the device scratch needed by xs_launch_smm_f64 for this call. */
 size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params);
@@ -65,14 +70,14 @@ size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_sm
 int xs_launch_smm_f64(const int* dev_stack, int stack_size, const double* a, const double* b, double* c, int m, int n,
   int k, const xs_smm_params_t* params, void* scratch, size_t scratch_bytes, void* stream);
 
-/** Stable grouping of a stack by c (stack_sort.cu): extract splits the AoS stack into keys (c) and
-    payload (a | b << 32), resets the segment list and gathers the bucket statistics; sort writes
-    the grouped order to (kout, vout) using (k0, v0) and (k1, v1) as ping-pong buffers. */
+/** Stable grouping of a stack by c (stack_sort.cu), one cooperative kernel: splits the AoS stack
+    into keys (c) and payload (a | b << 32) in (k0, v0), resets the segment list, and writes the
+    grouped order to (kout, vout), using (k1, v1) as ping-pong buffers for multi-pass sorts. */
 size_t xs_stack_sort_scratch_bytes(int S);
-int xs_stack_extract(const int* dev_stack, int S, unsigned* keys, unsigned long long* vals, int* seglist, void* sort_scratch,
-  void* stream);
-int xs_stack_sort(int S, unsigned* k0, unsigned long long* v0, unsigned* k1, unsigned long long* v1, unsigned* kout,
-  unsigned long long* vout, void* sort_scratch, void* stream);
+/** Largest stack xs_stack_group takes in one launch (larger stacks are processed in parts). */
+int xs_stack_group_max(void);
+int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
 /** Reads the sort's error flag (1 = a grid barrier timed out); synchronises the stream. */
 int xs_stack_sort_error(void* sort_scratch, int* err, void* stream);
 

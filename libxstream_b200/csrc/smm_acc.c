@@ -157,6 +157,7 @@ int libxstream_b200_set_params(int m, int n, int k, int chunk, int mt, int nt, i
   p.kp = kp;
   p.wpb = wpb;
   p.sorted = 0;
+  p.generic = 0;
   return xs_params_set((int)dbcsr_type_real_8, m, n, k, &p, 0.0);
 }
 

@@ -32,17 +32,22 @@ namespace {
 /* Warps of the combine kernel (its warp partials go through dynamic shared memory). */
 constexpr int kCombineWarps = 16;
 
+/* Bring a block of `count` contiguous doubles into L2 (one prefetch per 128-byte line, by 32 lanes). */
+__device__ __forceinline__ void prefetch_block_l2(const double* p, int count, int lane) {
+  for (int x = 16 * lane; x < count + 15; x += 16 * 32) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p + (x < count ? x : count - 1)));
+  }
+}
+
 __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
 
-/* Per-lane geometry of a warp sub-tile: which rows/cols of C (and of the A/B fragments) it owns. */
+/* Per-lane geometry of a warp sub-tile (8*MT x 8*NT of C): which fragment rows/columns it loads. */
 template <int MT, int NT>
 struct Tile {
-  int row[MT];  /* A row loaded for fragment tile i (g-th row of tile i) */
-  int col[NT];  /* B col loaded for fragment tile j */
   bool rok[MT], cok[NT];
   int r0, c0;
   __device__ __forceinline__ void init(int sub, int nsub_n, int m, int n, int g) {
@@ -50,51 +55,13 @@ struct Tile {
     r0 = sm * 8 * MT;
     c0 = sn * 8 * NT;
 #pragma unroll
-    for (int i = 0; i < MT; ++i) {
-      row[i] = r0 + 8 * i + g;
-      rok[i] = row[i] < m;
-    }
+    for (int i = 0; i < MT; ++i) rok[i] = r0 + 8 * i + g < m;
 #pragma unroll
-    for (int j = 0; j < NT; ++j) {
-      col[j] = c0 + 8 * j + g;
-      cok[j] = col[j] < n;
-    }
+    for (int j = 0; j < NT; ++j) cok[j] = c0 + 8 * j + g < n;
   }
 };
 
-template <int MT, int NT, int KP>
-__device__ __forceinline__ void load_panel(double (&fa)[KP][MT], double (&fb)[KP][NT], const double* __restrict__ A,
-  const double* __restrict__ B, unsigned long long v, int ks0, int t, int m, int n, int k, const Tile<MT, NT>& tl) {
-  const size_t aoff = (size_t)((unsigned)v) - 1, boff = (size_t)((unsigned)(v >> 32)) - 1;
-#pragma unroll
-  for (int p = 0; p < KP; ++p) {
-    const int kk = 4 * (ks0 + p) + t;
-    const bool okk = kk < k;
-    const double* const ap = A + aoff + (size_t)kk * m;
-    const double* const bp = B + boff + (size_t)kk * n;
-#pragma unroll
-    for (int i = 0; i < MT; ++i) fa[p][i] = (okk && tl.rok[i]) ? __ldg(ap + tl.row[i]) : 0.0;
-#pragma unroll
-    for (int j = 0; j < NT; ++j) fb[p][j] = (okk && tl.cok[j]) ? __ldg(bp + tl.col[j]) : 0.0;
-  }
-}
-
-template <int MT, int NT, int KP>
-__device__ __forceinline__ void mma_panel(double (&acc)[MT][NT][2], const double (&fa)[KP][MT], const double (&fb)[KP][NT],
-  int ks0, int KS) {
-#pragma unroll
-  for (int p = 0; p < KP; ++p) {
-    if (ks0 + p < KS) {
-#pragma unroll
-      for (int i = 0; i < MT; ++i) {
-#pragma unroll
-        for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], fa[p][i], fb[p][j]);
-      }
-    }
-  }
-}
-
-/* Write-back of a finished C sub-tile: each element has exactly one writer. */
+/* Write-back of a finished C sub-tile: each element has exactly one writer (red.global.add.f64). */
 template <int MT, int NT>
 __device__ __forceinline__ void commit_tile(double* __restrict__ C, size_t coff, const double (&acc)[MT][NT][2], int m,
   int n, int g, int t, const Tile<MT, NT>& tl) {
@@ -118,16 +85,23 @@ __host__ __device__ constexpr size_t smm_smem_bytes(int warps) {
   return (size_t)warps * (2 * MT * NT * 2 * 32 * sizeof(double) + 4 * sizeof(int));
 }
 
-/* The stack kernel. CTA = W warps = W consecutive chunks of L sorted entries, one warp sub-tile.
-   Segments inside a chunk are written back directly. Pieces of segments that cross chunk
-   boundaries are merged inside the CTA through shared memory (in warp order); only segments that
+/* Registers per thread the kernel may use: tiles up to 3x3 run 3 CTAs of 4 warps per SM. */
+__host__ __device__ constexpr int smm_min_blocks(int mt, int nt) { return (mt * nt <= 9) ? 3 : 2; }
+
+/* The stack kernel. M_, N_, K_ > 0 make the block shape a compile-time constant (every fragment
+   load is then one load at an immediate offset from a per-lane base pointer); 0 means runtime.
+   CTA = W warps = W consecutive chunks of L sorted entries, one warp sub-tile of C each. Per warp:
+   DMMA fragments of the next k-panel (KP k-steps of 4) are loaded while the current panel runs;
+   a segment that ends inside the chunk is written back at once; pieces of segments crossing chunk
+   boundaries are merged inside the CTA through shared memory in warp order, and only segments that
    cross the CTA's own boundaries leave a CTA-level piece in global scratch for the combine kernel. */
-template <int MT, int NT, int KP>
-__global__ void __launch_bounds__(128) xs_smm_dmma_kernel(const unsigned* __restrict__ keys,
+template <int M_, int N_, int K_, int MT, int NT, int KP>
+__global__ void __launch_bounds__(128, smm_min_blocks(MT, NT)) xs_smm_dmma_kernel(const unsigned* __restrict__ keys,
   const unsigned long long* __restrict__ vals, int S, const double* __restrict__ A, const double* __restrict__ B,
-  double* __restrict__ C, int m, int n, int k, int L, int nchunks, int nsub_n, int nsub, double* __restrict__ pieces,
-  int* __restrict__ seglist) {
+  double* __restrict__ C, int m_rt, int n_rt, int k_rt, int L, int nchunks, int nsub_n, int nsub,
+  double* __restrict__ pieces, int* __restrict__ seglist) {
   constexpr int REGS = MT * NT * 2;
+  const int m = M_ ? M_ : m_rt, n = N_ ? N_ : n_rt, k = K_ ? K_ : k_rt;
   extern __shared__ double smem[];
   const int W = blockDim.x >> 5;
   double* const sp = smem;                                       /* [W][2][REGS][32] */
@@ -135,9 +109,12 @@ __global__ void __launch_bounds__(128) xs_smm_dmma_kernel(const unsigned* __rest
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const int group = blockIdx.x / nsub, sub = blockIdx.x - group * nsub;
   const int chunk = group * W + warp;
-  const int KS = (k + 3) >> 2, npan = (KS + KP - 1) / KP;
+  const int KS = (k + 3) >> 2;
+  const int npan = (KS + KP - 1) / KP;
   Tile<MT, NT> tl;
   tl.init(sub, nsub_n, m, n, g);
+  const int klim = (k - t + 3) >> 2; /* k-steps in which this lane's k index is inside the block */
+  const unsigned a_lane = (unsigned)(t * m + tl.r0 + g), b_lane = (unsigned)(t * n + tl.c0 + g);
   if (0 == lane) {
     meta[warp * 4 + 0] = 0;
     meta[warp * 4 + 1] = 0;
@@ -155,13 +132,45 @@ __global__ void __launch_bounds__(128) xs_smm_dmma_kernel(const unsigned* __rest
 #pragma unroll
       for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
+    /* fragments of panel `pan` of the entry with payload v: A(row, 4ks+t) and B(4ks+t, col) */
+    auto load = [&](double (&fa)[KP][MT], double (&fb)[KP][NT], unsigned long long v, int pan) {
+      const double* const ap = A + ((unsigned)v - 1u + a_lane);
+      const double* const bp = B + ((unsigned)(v >> 32) - 1u + b_lane);
+#pragma unroll
+      for (int p = 0; p < KP; ++p) {
+        const int ks = pan * KP + p;
+        const bool ok = ks < klim;
+#pragma unroll
+        for (int i = 0; i < MT; ++i) fa[p][i] = (ok && tl.rok[i]) ? __ldg(ap + 4 * ks * m + 8 * i) : 0.0;
+#pragma unroll
+        for (int j = 0; j < NT; ++j) fb[p][j] = (ok && tl.cok[j]) ? __ldg(bp + 4 * ks * n + 8 * j) : 0.0;
+      }
+    };
+    auto mma = [&](const double (&fa)[KP][MT], const double (&fb)[KP][NT], int pan) {
+#pragma unroll
+      for (int p = 0; p < KP; ++p) {
+        if (pan * KP + p < KS) {
+#pragma unroll
+          for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], fa[p][i], fb[p][j]);
+        }
+      }
+    };
+
     double fa0[KP][MT], fb0[KP][NT], fa1[KP][MT], fb1[KP][NT];
+    /* payload pipeline: entry e (cur), e+1 (nxt), e+2 (nn); blocks of e+2 are prefetched into L2 */
     unsigned key_cur = keys[p0];
     unsigned long long v_cur = vals[p0];
     unsigned long long v_nxt = (p0 + 1 < p1) ? vals[p0 + 1] : 0ull;
+    unsigned long long v_nn = (p0 + 2 < p1) ? vals[p0 + 2] : 0ull;
     unsigned key_nxt = (p0 + 1 < p1) ? keys[p0 + 1] : 0u;
     int e = p0, pan = 0, segstart = p0;
-    load_panel<MT, NT, KP>(fa0, fb0, A, B, v_cur, 0, t, m, n, k, tl);
+    load(fa0, fb0, v_cur, 0);
+    if (p0 + 1 < p1) {
+      prefetch_block_l2(A + ((unsigned)v_nxt - 1u), m * k, lane);
+      prefetch_block_l2(B + ((unsigned)(v_nxt >> 32) - 1u), k * n, lane);
+    }
 
     /* One step: prefetch the next panel into (fan, fbn), run the current one from (fac, fbc),
        finish a segment when its last entry is done, advance. Returns false when the chunk is done. */
@@ -169,8 +178,8 @@ __global__ void __launch_bounds__(128) xs_smm_dmma_kernel(const unsigned* __rest
       const bool last_pan = (pan + 1 == npan);
       const int e2 = last_pan ? e + 1 : e;
       const int pan2 = last_pan ? 0 : pan + 1;
-      if (e2 < p1) load_panel<MT, NT, KP>(fan, fbn, A, B, last_pan ? v_nxt : v_cur, pan2 * KP, t, m, n, k, tl);
-      mma_panel<MT, NT, KP>(acc, fac, fbc, pan * KP, KS);
+      if (e2 < p1) load(fan, fbn, last_pan ? v_nxt : v_cur, pan2);
+      mma(fac, fbc, pan);
       if (last_pan) {
         const bool seg_end = (e + 1 == p1) || (key_nxt != key_cur);
         if (seg_end) {
@@ -207,8 +216,11 @@ __global__ void __launch_bounds__(128) xs_smm_dmma_kernel(const unsigned* __rest
           v_cur = v_nxt;
           key_cur = key_nxt;
           if (e + 2 < p1) {
-            v_nxt = vals[e + 2];
+            v_nxt = v_nn;
             key_nxt = keys[e + 2];
+            prefetch_block_l2(A + ((unsigned)v_nxt - 1u), m * k, lane);
+            prefetch_block_l2(B + ((unsigned)(v_nxt >> 32) - 1u), k * n, lane);
+            if (e + 3 < p1) v_nn = vals[e + 3];
           }
         }
       }
@@ -355,16 +367,33 @@ struct SmmPlan {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+typedef cudaError_t (*launch_fn_t)(const SmmPlan&, const unsigned*, const unsigned long long*, int, const double*,
+  const double*, double*, int, int, int, double*, int*, cudaStream_t, int*);
+
+launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm);
+
+/* Work decomposition and scratch layout of one call. An open chunk length (prm->chunk <= 0) is
+   sized so that the grid is one full wave of resident CTAs: L = ceil(S * nsub / (resident * W)). */
 int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl) {
-  (void)k;
   const int mt = prm->mt, nt = prm->nt;
-  if (mt < 1 || mt > 4 || nt < 1 || nt > 4 || prm->chunk < 1) return -1;
-  pl->L = prm->chunk;
+  if (mt < 1 || mt > 4 || nt < 1 || nt > 4) return -1;
   pl->nsub_m = ((m + 7) / 8 + mt - 1) / mt;
   pl->nsub_n = ((n + 7) / 8 + nt - 1) / nt;
   pl->nsub = pl->nsub_m * pl->nsub_n;
-  pl->nchunks = (S + pl->L - 1) / pl->L;
   pl->W = (prm->wpb >= 1 && prm->wpb <= 4) ? prm->wpb : 4;
+  if (0 < prm->chunk) pl->L = prm->chunk;
+  else {
+    int occ = 0;
+    const launch_fn_t fn = find_launcher(m, n, k, prm);
+    if (cudaSuccess != fn(*pl, nullptr, nullptr, 0, nullptr, nullptr, nullptr, m, n, k, nullptr, nullptr, 0, &occ) ||
+        occ < 1) {
+      occ = 1;
+    }
+    const long resident = (long)occ * xs_sm_count();
+    const long L = ((long)S * pl->nsub + resident * pl->W - 1) / (resident * pl->W);
+    pl->L = (int)(L < 1 ? 1 : L);
+  }
+  pl->nchunks = (S + pl->L - 1) / pl->L;
   pl->ngroups = (pl->nchunks + pl->W - 1) / pl->W;
   size_t off = 0;
   const size_t ks = align_up(sizeof(unsigned) * (size_t)S, 256), vs = align_up(sizeof(unsigned long long) * (size_t)S, 256);
@@ -390,19 +419,25 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   return 0;
 }
 
-template <int MT, int NT, int KP>
+/* Launches the stack kernel and the combine kernel for one planned call. With occ != nullptr it
+   only reports how many CTAs of W = pl.W warps fit on one SM (the plan sizes chunks from that). */
+template <int M_, int N_, int K_, int MT, int NT, int KP>
 cudaError_t launch_dmma(const SmmPlan& pl, const unsigned* keys, const unsigned long long* vals, int S, const double* a,
-  const double* b, double* c, int m, int n, int k, double* pieces, int* seglist, cudaStream_t s) {
+  const double* b, double* c, int m, int n, int k, double* pieces, int* seglist, cudaStream_t s, int* occ) {
   cudaError_t r;
   static int smem_set = 0, csmem_set = 0; /* per template instance; setting them twice is harmless */
   const size_t smem = smm_smem_bytes<MT, NT>(pl.W);
   if (smem > 48 * 1024 && smem_set < (int)smem) {
-    r = cudaFuncSetAttribute(xs_smm_dmma_kernel<MT, NT, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    r = cudaFuncSetAttribute(xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)smem);
     if (cudaSuccess != r) return r;
     smem_set = (int)smem;
   }
+  if (nullptr != occ) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, 32 * pl.W, smem);
+  }
   void* prof = xs_profile_begin(s);
-  xs_smm_dmma_kernel<MT, NT, KP><<<pl.ngroups * pl.nsub, 32 * pl.W, smem, s>>>(
+  xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP><<<pl.ngroups * pl.nsub, 32 * pl.W, smem, s>>>(
     keys, vals, S, a, b, c, m, n, k, pl.L, pl.nchunks, pl.nsub_n, pl.nsub, pieces, seglist);
   r = cudaGetLastError();
   if (cudaSuccess != r) return r;
@@ -423,16 +458,36 @@ cudaError_t launch_dmma(const SmmPlan& pl, const unsigned* keys, const unsigned 
   return r;
 }
 
-typedef cudaError_t (*launch_fn_t)(const SmmPlan&, const unsigned*, const unsigned long long*, int, const double*,
-  const double*, double*, int, int, int, double*, int*, cudaStream_t);
-
-#define XS_KP_ENTRY(MT, NT) {&launch_dmma<MT, NT, 2>, &launch_dmma<MT, NT, 4>}
+/* Runtime-shape kernels: any (m, n, k), warp sub-tile MT x NT, KP in {2, 4}. */
+#define XS_KP_ENTRY(MT, NT) {&launch_dmma<0, 0, 0, MT, NT, 2>, &launch_dmma<0, 0, 0, MT, NT, 4>}
 static const launch_fn_t launch_table[4][4][2] = {
   {XS_KP_ENTRY(1, 1), XS_KP_ENTRY(1, 2), XS_KP_ENTRY(1, 3), XS_KP_ENTRY(1, 4)},
   {XS_KP_ENTRY(2, 1), XS_KP_ENTRY(2, 2), XS_KP_ENTRY(2, 3), XS_KP_ENTRY(2, 4)},
   {XS_KP_ENTRY(3, 1), XS_KP_ENTRY(3, 2), XS_KP_ENTRY(3, 3), XS_KP_ENTRY(3, 4)},
   {XS_KP_ENTRY(4, 1), XS_KP_ENTRY(4, 2), XS_KP_ENTRY(4, 3), XS_KP_ENTRY(4, 4)},
 };
+
+/* Shape-specialised kernels for the square block sizes DBCSR workloads use most. */
+struct SpecEntry {
+  int m, n, k, mt, nt, kp;
+  launch_fn_t fn;
+};
+#define XS_SPEC(S, MT, KP) {S, S, S, MT, MT, KP, &launch_dmma<S, S, S, MT, MT, KP>}
+static const SpecEntry spec_table[] = {
+  XS_SPEC(4, 1, 1), XS_SPEC(5, 1, 2), XS_SPEC(8, 1, 2), XS_SPEC(9, 2, 3), XS_SPEC(13, 2, 2), XS_SPEC(13, 2, 4),
+  XS_SPEC(16, 2, 2), XS_SPEC(16, 2, 4), XS_SPEC(22, 3, 2), XS_SPEC(22, 3, 3), XS_SPEC(23, 3, 2), XS_SPEC(23, 3, 3),
+  XS_SPEC(26, 4, 2), XS_SPEC(26, 4, 4), XS_SPEC(32, 4, 2), XS_SPEC(32, 4, 4), XS_SPEC(45, 3, 2), XS_SPEC(45, 3, 4),
+  XS_SPEC(64, 4, 2), XS_SPEC(64, 4, 4),
+};
+
+launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
+  if (0 == prm->generic) {
+    for (const SpecEntry& e : spec_table) {
+      if (e.m == m && e.n == n && e.k == k && e.mt == prm->mt && e.nt == prm->nt && e.kp == prm->kp) return e.fn;
+    }
+  }
+  return launch_table[prm->mt - 1][prm->nt - 1][(4 == prm->kp) ? 1 : 0];
+}
 
 /* ------------------------------------------------------------------------------ transpose */
 
@@ -492,8 +547,24 @@ __global__ void xs_dmma_peak_kernel(double* out, int iters) {
 
 extern "C" {
 
+int xs_smm_f64_specialized(int m, int n, int k, int* mt_kp_pairs, int capacity) {
+  int count = 0;
+  for (const SpecEntry& e : spec_table) {
+    if (e.m == m && e.n == n && e.k == k) {
+      if (count < capacity && nullptr != mt_kp_pairs) {
+        mt_kp_pairs[3 * count + 0] = e.mt;
+        mt_kp_pairs[3 * count + 1] = e.nt;
+        mt_kp_pairs[3 * count + 2] = e.kp;
+      }
+      ++count;
+    }
+  }
+  return count;
+}
+
 size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params) {
   SmmPlan pl;
+  if (stack_size > xs_stack_group_max()) stack_size = xs_stack_group_max(); /* processed in parts */
   if (0 >= stack_size || 0 != plan_smm(stack_size, m, n, k, params, &pl)) return 0;
   return pl.total;
 }
@@ -503,6 +574,15 @@ int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double
   SmmPlan pl;
   cudaStream_t s = (cudaStream_t)stream;
   if (0 >= S) return 0;
+  const int smax = xs_stack_group_max();
+  if (S > smax) { /* C += A*B is additive over the stack: run it in consecutive parts */
+    for (int off = 0; off < S; off += smax) {
+      const int r = xs_launch_smm_f64(dev_stack + 3 * (size_t)off, min(smax, S - off), a, b, c, m, n, k, prm, scratch,
+        scratch_bytes, stream);
+      if (0 != r) return r;
+    }
+    return 0;
+  }
   if (0 != plan_smm(S, m, n, k, prm, &pl) || scratch_bytes < pl.total || nullptr == scratch) return (int)cudaErrorInvalidValue;
   char* const base = (char*)scratch;
   unsigned* const keys_in = (unsigned*)(base + pl.off_keys_in);
@@ -515,22 +595,14 @@ int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double
   double* const pieces = (double*)(base + pl.off_pieces);
   void* const sort_scratch = base + pl.off_sort;
   void* prof = xs_profile_begin(s);
-  int r = xs_stack_extract(dev_stack, S, keys_in, vals_in, seglist, sort_scratch, s);
+  const int r = xs_stack_group(dev_stack, S, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, seglist,
+    sort_scratch, s);
   if (0 != r) return r;
-  xs_profile_end(prof, "extract", 0.0, 24.0 * S, s);
-  const unsigned* keys = keys_in;
-  const unsigned long long* vals = vals_in;
-  if (!prm->sorted) {
-    prof = xs_profile_begin(s);
-    r = xs_stack_sort(S, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, sort_scratch, s);
-    if (0 != r) return r;
-    xs_profile_end(prof, "sort", 0.0, 24.0 * S, s);
-    keys = keys_out;
-    vals = vals_out;
-  }
-  const int kp = (4 == prm->kp) ? 1 : 0;
-  const launch_fn_t fn = launch_table[prm->mt - 1][prm->nt - 1][kp];
-  return (int)fn(pl, keys, vals, S, a, b, c, m, n, k, pieces, seglist, s);
+  xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
+  const unsigned* const keys = keys_out;
+  const unsigned long long* const vals = vals_out;
+  const launch_fn_t fn = find_launcher(m, n, k, prm);
+  return (int)fn(pl, keys, vals, S, a, b, c, m, n, k, pieces, seglist, s, nullptr);
 }
 
 int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize, int m, int n, void* stream) {

@@ -35,10 +35,11 @@ static unsigned xs_hash(int type, int m, int n, int k) {
 static int xs_clamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 static void xs_sanitize(xs_smm_params_t* p) {
-  p->chunk = xs_clamp(p->chunk, 1, 4096);
+  p->chunk = xs_clamp(p->chunk, 0, 1 << 20); /* 0: sized per stack by the launcher */
   p->mt = xs_clamp(p->mt, 1, 4);
   p->nt = xs_clamp(p->nt, 1, 4);
-  p->kp = (4 == p->kp) ? 4 : 2;
+  p->kp = xs_clamp(p->kp, 1, 4);
+  p->generic = (0 != p->generic) ? 1 : 0;
   p->wpb = xs_clamp(p->wpb, 1, 4);
   p->sorted = (0 != p->sorted) ? 1 : 0;
 }
@@ -60,20 +61,25 @@ static int xs_pick_tiles(int dim) {
 }
 
 void xs_params_default(int m, int n, int k, int stack_size, xs_smm_params_t* out) {
-  const int sms = xs_sm_count();
   const int mt = xs_pick_tiles(m), nt = xs_pick_tiles(n);
-  const int nsub = ((((m + 7) / 8) + mt - 1) / mt) * ((((n + 7) / 8) + nt - 1) / nt);
-  /* about 16 resident warps per SM in one wave; never fewer than 4 entries per warp */
-  const long target_items = (long)sms * 16;
-  long chunk = ((long)stack_size * nsub + target_items - 1) / target_items;
-  (void)k;
-  if (chunk < 4) chunk = 4;
-  out->chunk = (int)chunk;
+  (void)stack_size;
+  out->chunk = 0; /* open: the launcher sizes chunks to one wave of resident CTAs */
   out->mt = mt;
   out->nt = nt;
   out->kp = ((k + 3) / 4 <= 2) ? 2 : 4;
   out->wpb = 4;
   out->sorted = 0;
+  out->generic = 0;
+  { /* prefer a shape-specialised kernel with the same tiles (the first one listed) */
+    int triples[3 * 8], i;
+    const int nspec = xs_smm_f64_specialized(m, n, k, triples, 8);
+    for (i = 0; i < nspec && i < 8; ++i) {
+      if (triples[3 * i] == mt && triples[3 * i + 1] == nt) {
+        out->kp = triples[3 * i + 2];
+        break;
+      }
+    }
+  }
   xs_sanitize(out);
 }
 
@@ -92,11 +98,6 @@ void xs_params_lookup(int type, int m, int n, int k, int stack_size, xs_smm_para
   }
   pthread_rwlock_unlock(&xs_table_lock);
   if (!found) xs_params_default(m, n, k, stack_size, out);
-  else if (0 >= out->chunk) { /* a record may leave L open: size it to the stack */
-    xs_smm_params_t d;
-    xs_params_default(m, n, k, stack_size, &d);
-    out->chunk = d.chunk;
-  }
 }
 
 int xs_params_set(int type, int m, int n, int k, const xs_smm_params_t* p, double gflops) {
@@ -115,7 +116,6 @@ int xs_params_set(int type, int m, int n, int k, const xs_smm_params_t* p, doubl
         r->gflops = gflops;
         r->p = *p;
         xs_sanitize(&r->p);
-        if (0 >= p->chunk) r->p.chunk = 0; /* L left open: sized to each stack at lookup */
       }
       result = 0;
       break;
@@ -131,7 +131,7 @@ void xs_params_clear(void) {
   pthread_rwlock_unlock(&xs_table_lock);
 }
 
-/* CSV: DEVICE;TYPEID;M;N;K;S;GFLOPS;L;MT;NT;KP;WPB (the first line is a header). */
+/* CSV: DEVICE;TYPEID;M;N;K;S;GFLOPS;L;MT;NT;KP;WPB[;GEN] (the first line is a header). */
 int xs_params_load_csv(const char* path) {
   char line[1024];
   int count = 0, lineno = 0;
@@ -157,6 +157,7 @@ int xs_params_load_csv(const char* path) {
       p.kp = atoi(fields[10]);
       p.wpb = atoi(fields[11]);
       p.sorted = 0;
+      p.generic = (13 <= nf) ? atoi(fields[12]) : 0;
       if (0 < m && 0 < n && 0 < k && 0 == xs_params_set(type, m, n, k, &p, gflops)) ++count;
     }
   }
