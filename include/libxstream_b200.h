@@ -72,6 +72,24 @@ int libxstream_b200_graph_end(void* stream, void** graph_exec, int* nkernels);
 int libxstream_b200_graph_launch(void* graph_exec, void* stream);
 int libxstream_b200_graph_destroy(void* graph_exec);
 
+/** Allocation-free stack multiply, for callers that cannot let the library allocate device memory
+    per call: applications that reserve nearly all device memory for their own allocator at
+    start-up, or code that must not take the driver's allocation locks or risk the device
+    synchronisation a growing memory pool or cudaFree can cause. Same arguments, results and
+    return codes as libsmm_acc_process; its scratch is a fixed 8 MiB device array inside the
+    library (held by every GPU that uses the library until the process exits), so a stack that
+    needs more (libxstream_b200_process_scratch_bytes) is rejected with a nonzero return and a
+    message. The first call on a device looks up the array's device address: make it before any
+    stream capture. All calls on a device share the array; calls that overlap on the GPU race and
+    must be ordered by the caller. This entry point has no counterpart in the reference. */
+int libxstream_b200_process_noalloc(const int* host_param_stack, const int* dev_param_stack, int stack_size,
+  libsmm_acc_data_t datatype, const void* dev_a_data, const void* dev_b_data, void* dev_c_data, int m_max, int n_max,
+  int k_max, int max_kernel_dim, c_dbcsr_acc_bool_t def_mnk, void* stack_stream, void* c_stream);
+/** Size of the allocation-free entry point's scratch array (8 MiB), and the scratch a stack of
+    stack_size (m, n, k) FP64 entries needs with the current parameters (0 for an invalid shape). */
+size_t libxstream_b200_noalloc_scratch_bytes(void);
+size_t libxstream_b200_process_scratch_bytes(int stack_size, int m, int n, int k);
+
 #if defined(__cplusplus)
 }
 #endif

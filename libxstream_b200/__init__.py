@@ -83,6 +83,12 @@ SIGNATURES = {
     "libxstream_b200_graph_end": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_int_p]),
     "libxstream_b200_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "libxstream_b200_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "libxstream_b200_process_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                       ctypes.c_void_p, ctypes.c_void_p]),
+    "libxstream_b200_noalloc_scratch_bytes": (ctypes.c_size_t, []),
+    "libxstream_b200_process_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
 }
 
 DBCSR_TYPE_REAL_4 = 1

@@ -65,6 +65,8 @@ static int xs_lazy_init(void) {
   return result;
 }
 
+int xs_smm_ensure_init(void) { return xs_lazy_init(); }
+
 int libxstream_b200_process_suitable(
   c_dbcsr_acc_bool_t def_mnk, libsmm_acc_data_t datatype, int stack_size, int m, int n, int k, int max_kernel_dim) {
   const long mn = (long)m * n;
