@@ -25,9 +25,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -89,68 +87,80 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while the benchmark runs."""
+    """SM clock, power and clock-event reasons sampled every 20 ms by an NVML thread while the
+    benchmark runs (read-only queries)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.proc = None
+        self.samples = []
+        self.stop_flag = False
+        self.thread = None
+        self.error = None
+
+    def _run(self):
+        import pynvml as N
+        try:
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            while not self.stop_flag:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                try:
+                    reasons = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except AttributeError:
+                    reasons = N.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                power = N.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append((sm, reasons, power))
+                time.sleep(0.02)
+            N.nvmlShutdown()
+        except Exception as exc:  # NVML missing or not permitted: report it, do not fail the run
+            self.error = str(exc)
 
     def start(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
-                                         stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+        import threading
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.file.flush()
-        rows = []
-        for line in Path(self.file.name).read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.file.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        self.stop_flag = True
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "no samples"], "samples": 0}
+        import pynvml as N
+        busy = [x for x in self.samples if x[2] > 200.0] or self.samples  # under load (> 200 W)
+        names = sorted({name for name, const in self.REASONS for _, r, _ in busy
+                        if hasattr(N, const) and (r & getattr(N, const))})
+        return {"sm_mhz": statistics.median(x[0] for x in busy), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples), "samples_under_load": len(busy),
+                "power_w_max": max(x[2] for x in self.samples)}
 
 
 def cpu_baseline(case, seconds: float) -> dict:
-    """Oracle restatement of the reference's host SMM path, all host threads, bounded sample."""
+    """The reference's host SMM path restated (register-tiled FMA kernel, all host threads), timed
+    on a bounded sample of repetitions of the full stack."""
     import oracle
     threads = oracle.max_threads()
     c = np.zeros(case.nc * case.m * case.n)
     for _ in range(2):  # warm-up, like acc_bench.c:366-377
-        oracle.smm(case.stack, case.a, case.b, c, case.m, case.n, case.k, b_rowmajor=False, threads=threads)
+        oracle.smm_fast(case.stack, case.a, case.b, c, case.m, case.n, case.k, threads=threads)
     reps = 0
     t0 = time.perf_counter()
     while True:
-        oracle.smm(case.stack, case.a, case.b, c, case.m, case.n, case.k, b_rowmajor=False, threads=threads)
+        oracle.smm_fast(case.stack, case.a, case.b, c, case.m, case.n, case.k, threads=threads)
         reps += 1
         el = time.perf_counter() - t0
         if el >= seconds:
             break
     return {"value": case.flops * reps / el * 1e-9, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{reps} repetitions of the full {case.m}x{case.n}x{case.k} stack ({case.S} triples), "
-                      f"{el:.1f} s, OpenMP restatement (oracle/smm_oracle.c)"}
+                      f"{el:.1f} s, OpenMP register-tiled restatement (oracle/smm_oracle.c: oracle_smm_f64_fast)"}
 
 
 def workload_config(case) -> dict:
@@ -170,11 +180,11 @@ def run_reference(args, d: Dist):
     threads = oracle.max_threads()
     c = np.zeros(case.nc * case.m * case.n)
     for _ in range(max(args.warmup, 3)):
-        oracle.smm(case.stack, case.a, case.b, c, case.m, case.n, case.k, b_rowmajor=False, threads=threads)
+        oracle.smm_fast(case.stack, case.a, case.b, c, case.m, case.n, case.k, threads=threads)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        oracle.smm(case.stack, case.a, case.b, c, case.m, case.n, case.k, b_rowmajor=False, threads=threads)
+        oracle.smm_fast(case.stack, case.a, case.b, c, case.m, case.n, case.k, threads=threads)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
     value = case.flops / (ms * 1e-3) * 1e-9

@@ -28,6 +28,8 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_int]
         _lib.oracle_smm_f64_omp.argtypes = [_ip, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _lib.oracle_smm_f64_fast.argtypes = [_ip, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int]
         _lib.oracle_transpose_f64.argtypes = [_ip, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int]
         _lib.oracle_norms.argtypes = [_dp, ctypes.c_int, _ip, _ip, ctypes.POINTER(ctypes.c_float)]
         _lib.oracle_block_relerr.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int]
@@ -58,6 +60,16 @@ def smm(stack: np.ndarray, a: np.ndarray, b: np.ndarray, c: np.ndarray, m: int, 
     else:
         lib().oracle_smm_f64_omp(_p(stack, ctypes.c_int), S, _p(a, ctypes.c_double), _p(b, ctypes.c_double),
                                  _p(c, ctypes.c_double), m, n, k, int(b_rowmajor), int(threads))
+    return c
+
+
+def smm_fast(stack: np.ndarray, a: np.ndarray, b: np.ndarray, c: np.ndarray, m: int, n: int, k: int,
+             threads: int = 0) -> np.ndarray:
+    """Timed CPU baseline (register-tiled, FMA, all threads; B column-major): C += A*B in place."""
+    stack = np.ascontiguousarray(stack, dtype=np.int32)
+    assert a.dtype == b.dtype == c.dtype == np.float64 and c.flags.c_contiguous
+    lib().oracle_smm_f64_fast(_p(stack, ctypes.c_int), stack.size // 3, _p(a, ctypes.c_double), _p(b, ctypes.c_double),
+                              _p(c, ctypes.c_double), m, n, k, int(threads))
     return c
 
 
@@ -106,5 +118,5 @@ def ozaki_gemm(A: np.ndarray, B: np.ndarray, C: np.ndarray, M: int, N: int, K: i
     return C
 
 
-__all__ = ["lib", "smm", "transpose", "norms", "block_relerr", "max_threads", "ozaki_slice", "ozaki_gemm", "OUT",
+__all__ = ["lib", "smm", "smm_fast", "transpose", "norms", "block_relerr", "max_threads", "ozaki_slice", "ozaki_gemm", "OUT",
            "Path"]

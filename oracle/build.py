@@ -19,7 +19,7 @@ def build(force: bool = False) -> Path:
         return OUT
     OUT.parent.mkdir(exist_ok=True)
     tmp = OUT.with_suffix(".so.tmp")
-    cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+    cmd = ["gcc", "-O3", "-march=native", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
            "-Wall", "-o", str(tmp), str(SRC), "-lm"]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:

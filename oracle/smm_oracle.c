@@ -74,6 +74,95 @@ void oracle_smm_f64_omp(const int* stack, int S, const double* a, const double* 
 #endif
 }
 
+/* One triple with B column-major (ldb = k, the host contract of acc_bench.c:369-374) for the timed
+   baseline: an 8 x 4 register tile of C (generic GCC vectors of 4 doubles, fused multiply-adds) over
+   the rows in steps of 8, a scalar loop for the remaining rows -- the structure of a tuned host
+   small-GEMM kernel such as the LIBXS JIT kernels the reference's host path runs. */
+typedef double xs_v4d __attribute__((vector_size(32)));
+
+__attribute__((optimize("fp-contract=fast"))) static void smm_entry_fast(const double* a, const double* b, double* c,
+  int m, int n, int k) {
+  int i0 = 0, j0, jj, kk, i;
+  for (; i0 + 8 <= m; i0 += 8) {
+    for (j0 = 0; j0 < n; j0 += 4) {
+      const int nj = (n - j0 < 4) ? n - j0 : 4;
+      xs_v4d acc[4][2];
+      for (jj = 0; jj < 4; ++jj) {
+        if (jj < nj) {
+          memcpy(&acc[jj][0], c + (size_t)(j0 + jj) * m + i0, sizeof(xs_v4d));
+          memcpy(&acc[jj][1], c + (size_t)(j0 + jj) * m + i0 + 4, sizeof(xs_v4d));
+        }
+        else acc[jj][0] = acc[jj][1] = (xs_v4d){0, 0, 0, 0};
+      }
+      if (4 == nj) {
+        for (kk = 0; kk < k; ++kk) {
+          xs_v4d a0, a1;
+          memcpy(&a0, a + (size_t)kk * m + i0, sizeof(a0));
+          memcpy(&a1, a + (size_t)kk * m + i0 + 4, sizeof(a1));
+          for (jj = 0; jj < 4; ++jj) {
+            const double bv = b[(size_t)(j0 + jj) * k + kk];
+            acc[jj][0] += a0 * bv;
+            acc[jj][1] += a1 * bv;
+          }
+        }
+      }
+      else {
+        for (kk = 0; kk < k; ++kk) {
+          xs_v4d a0, a1;
+          memcpy(&a0, a + (size_t)kk * m + i0, sizeof(a0));
+          memcpy(&a1, a + (size_t)kk * m + i0 + 4, sizeof(a1));
+          for (jj = 0; jj < nj; ++jj) {
+            const double bv = b[(size_t)(j0 + jj) * k + kk];
+            acc[jj][0] += a0 * bv;
+            acc[jj][1] += a1 * bv;
+          }
+        }
+      }
+      for (jj = 0; jj < nj; ++jj) {
+        memcpy(c + (size_t)(j0 + jj) * m + i0, &acc[jj][0], sizeof(xs_v4d));
+        memcpy(c + (size_t)(j0 + jj) * m + i0 + 4, &acc[jj][1], sizeof(xs_v4d));
+      }
+    }
+  }
+  if (i0 < m) { /* remaining rows */
+    int j;
+    for (j = 0; j < n; ++j) {
+      double* const cj = c + (size_t)j * m;
+      const double* const bj = b + (size_t)j * k;
+      for (kk = 0; kk < k; ++kk) {
+        const double bv = bj[kk];
+        const double* const ak = a + (size_t)kk * m;
+        for (i = i0; i < m; ++i) cj[i] += ak[i] * bv;
+      }
+    }
+  }
+}
+
+/* Timed CPU baseline: the host SMM path with all threads (B column-major). Thread t owns
+   the C blocks whose offset hashes to t, so each block is still updated in stack order by one
+   thread; results differ from oracle_smm_f64 only by FMA rounding. */
+void oracle_smm_f64_fast(const int* stack, int S, const double* a, const double* b, double* c, int m, int n, int k,
+  int nthreads) {
+#if defined(_OPENMP)
+  if (0 >= nthreads) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+  {
+    const int nt = omp_get_num_threads(), tid = omp_get_thread_num();
+    int s;
+    for (s = 0; s < S; ++s) {
+      const unsigned cblk = (unsigned)(stack[3 * s + 2] - 1) / (unsigned)(m * n);
+      if ((int)((cblk * 2654435761u) % (unsigned)nt) == tid) {
+        smm_entry_fast(a + stack[3 * s] - 1, b + stack[3 * s + 1] - 1, c + stack[3 * s + 2] - 1, m, n, k);
+      }
+    }
+  }
+#else
+  int s;
+  (void)nthreads;
+  for (s = 0; s < S; ++s) smm_entry_fast(a + stack[3 * s] - 1, b + stack[3 * s + 1] - 1, c + stack[3 * s + 2] - 1, m, n, k);
+#endif
+}
+
 int oracle_max_threads(void) {
 #if defined(_OPENMP)
   return omp_get_max_threads();

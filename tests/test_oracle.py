@@ -42,6 +42,18 @@ def test_oracle_threads_bitwise_equal():
     assert np.array_equal(c1, c2)
 
 
+@pytest.mark.parametrize("shape", [(23, 23, 23), (5, 5, 5), (45, 45, 45), (9, 13, 7), (64, 3, 80)])
+def test_timed_baseline_matches_checker(shape):
+    """The timed CPU baseline (register-tiled, FMA) agrees with the exact checker to 1e-13."""
+    m, n, k = shape
+    case = W.stack_case(m, n, k, 2000, 80, 80, 30, seed=12)
+    ref = np.zeros(case.nc * m * n)
+    fast = np.zeros_like(ref)
+    oracle.smm(case.stack, case.a, case.b, ref, m, n, k, b_rowmajor=False)
+    oracle.smm_fast(case.stack, case.a, case.b, fast, m, n, k, threads=4)
+    assert oracle.block_relerr(fast, ref, m * n) < 1e-13
+
+
 def test_oracle_transpose_numpy():
     g = W.rng(5)
     m, n = 7, 5
