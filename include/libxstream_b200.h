@@ -12,10 +12,37 @@
 extern "C" {
 #endif
 
+/** One homogeneous FP64 stack of a batch: stack_size (a, b, c) triples of 1-based element offsets
+    (device memory) into the pools a, b (B already transposed, k x n row-major) and c, as for
+    libsmm_acc_process. */
+typedef struct libxstream_b200_stack_t {
+  const int* dev_param_stack;
+  int stack_size;
+  int m, n, k;
+  const void* a;
+  const void* b;
+  void* c;
+} libxstream_b200_stack_t;
+
+/** All stacks of one multiplication in one call: equivalent to one libsmm_acc_process per stack
+    (FP64, homogeneous, def_mnk = 1), but grouped together and run by one persistent stack kernel
+    whose CTAs take work items from all stacks, heaviest first, plus one combine kernel; the call is
+    capturable in a CUDA graph (libxstream_b200_graph_begin/end). Stacks may share pools; if two
+    stacks update the same C block their contributions are added atomically (correct, but not
+    bitwise reproducible). Returns -1 (nothing done) if any stack is one libsmm_acc_process would not
+    handle (m*n > max_kernel_dim^2, nonpositive sizes), else 0 or a CUDA error. No counterpart in the
+    reference, which launches one homogeneous stack per call (samples/smm/smm_acc.c:575-593). */
+int libxstream_b200_process_batch(const libxstream_b200_stack_t* stacks, int nstacks, int max_kernel_dim, void* stream);
+
 /** The suitability rule of libsmm_acc_process: 1 if the stack is handled on the GPU, else 0.
     Replaces libsmm_acc_process_suitable (samples/smm/smm_acc.c:527-573). */
 int libxstream_b200_process_suitable(
   c_dbcsr_acc_bool_t def_mnk, libsmm_acc_data_t datatype, int stack_size, int m, int n, int k, int max_kernel_dim);
+
+/** Device-side error word of the library (bit 0: a grid barrier of the grouping sort timed out, the
+    affected call then wrote nothing); reset != 0 clears it. Synchronises the device. No counterpart
+    in the reference. */
+int libxstream_b200_device_error(int reset);
 
 /** Last CUDA error code recorded by the library (0 if none); cleared by c_dbcsr_acc_clear_errors.
     Corresponds to the reference's error slot (libxstream/libxstream_opencl.h:156-194). */

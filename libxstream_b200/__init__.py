@@ -88,6 +88,8 @@ SIGNATURES = {
                                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                        ctypes.c_void_p, ctypes.c_void_p]),
     "libxstream_b200_noalloc_scratch_bytes": (ctypes.c_size_t, []),
+    "libxstream_b200_process_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "libxstream_b200_device_error": (ctypes.c_int, [ctypes.c_int]),
     "libxstream_b200_process_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
 }
 
@@ -97,6 +99,13 @@ DBCSR_TYPE_REAL_8 = 3
 
 class LibraryMissing(RuntimeError):
     pass
+
+
+class StackDesc(ctypes.Structure):
+    """libxstream_b200_stack_t (include/libxstream_b200.h): one stack of a batch."""
+    _fields_ = [("dev_param_stack", ctypes.c_void_p), ("stack_size", ctypes.c_int), ("m", ctypes.c_int),
+                ("n", ctypes.c_int), ("k", ctypes.c_int), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p),
+                ("c", ctypes.c_void_p)]
 
 
 def lib() -> ctypes.CDLL:

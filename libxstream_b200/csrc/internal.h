@@ -72,16 +72,49 @@ size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_sm
 int xs_launch_smm_f64(const int* dev_stack, int stack_size, const double* a, const double* b, double* c, int m, int n,
   int k, const xs_smm_params_t* params, void* scratch, size_t scratch_bytes, void* stream);
 
-/** Stable grouping of a stack by c (stack_sort.cu), one cooperative kernel: splits the AoS stack
-    into keys (c) and payload (a | b << 32) in (k0, v0), resets the segment list, and writes the
-    grouped order to (kout, vout), using (k1, v1) as ping-pong buffers for multi-pass sorts. */
+/** Stable grouping of stacks by c (stack_sort.cu), one cooperative kernel for one stack or a batch:
+    splits each AoS stack into keys (c) and payload (a | b << 32), resets the segment list, and
+    writes each stack's grouped order to (kout, vout) at its offset off[s], using (k0, v0) and
+    (k1, v1) as ping-pong buffers for multi-pass sorts. */
+#define XS_MAX_BATCH 16       /* stacks per grouping launch */
+#define XS_MAX_CALL_STACKS 64 /* stacks per library call (statistics slots in the control block) */
+typedef struct xs_sort_batch_t {
+  int nstacks;
+  int gidx[XS_MAX_BATCH];       /* index of the stack within the call (statistics slot) */
+  const int* stack[XS_MAX_BATCH];
+  int S[XS_MAX_BATCH];          /* entries per stack (>= 1) */
+  int off[XS_MAX_BATCH];        /* first output position of each stack */
+  int tile_begin[XS_MAX_BATCH]; /* filled by the launcher */
+  int ntiles[XS_MAX_BATCH];     /* filled by the launcher */
+} xs_sort_batch_t;
+size_t xs_sort_ctl_bytes(void);
+/** Zero the call's control block (barrier, error flag, queue, statistics of nstacks stacks). */
+int xs_sort_clear_ctl(void* sort_scratch, int nstacks, void* stream);
+/** Tiles one grouping launch takes at most, and entries per tile (small / large tiles). */
+int xs_sort_launch_tiles(void);
+int xs_sort_tile_entries(int large);
 size_t xs_stack_sort_scratch_bytes(int S);
-/** Largest stack xs_stack_group takes in one launch (larger stacks are processed in parts). */
+size_t xs_stack_sort_scratch_bytes_batch(const xs_sort_batch_t* desc);
+/** Largest single stack xs_stack_group takes in one launch (larger stacks are processed in parts). */
 int xs_stack_group_max(void);
+/** 1 if the batch fits one grouping launch. */
+int xs_stack_group_fits(const xs_sort_batch_t* desc);
+/** Grouping of a batch that fits one launch; the control block must have been cleared for the call
+    (xs_sort_clear_ctl) before the first launch of the call. */
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
-/** Reads the sort's error flag (1 = a grid barrier timed out); synchronises the stream. */
-int xs_stack_sort_error(void* sort_scratch, int* err, void* stream);
+int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
+/** Device addresses inside the sort scratch: the work-queue counter (zeroed with the statistics
+    at every call) and the error flag a timed-out grid barrier sets. */
+unsigned* xs_sort_queue_counter(void* sort_scratch);
+const unsigned* xs_sort_error_flag(void* sort_scratch);
+
+/** Batch of stacks (include/libxstream_b200.h: libxstream_b200_stack_t): scratch size and launch. */
+struct libxstream_b200_stack_t;
+size_t xs_smm_batch_scratch_bytes(const struct libxstream_b200_stack_t* stacks, int nstacks);
+int xs_launch_smm_batch(const struct libxstream_b200_stack_t* stacks, int nstacks, void* scratch, size_t scratch_bytes,
+  void* stream);
 
 /** In-place batched transpose of m x n blocks (element size esize: 4 or 8). Returns cudaError_t. */
 int xs_launch_transpose(const int* dev_trs_stack, int offset, int stack_size, void* data, int esize, int m, int n,

@@ -144,6 +144,43 @@ int c_calculate_norms(const double* mat, int nblks, const int* offsets, const in
 
 /* ------------------------------------------------------------------- extension entry points */
 
+static int xs_process_batch_part(const libxstream_b200_stack_t* stacks, int nstacks, void* stream) {
+  void* scratch = NULL;
+  size_t nbytes = xs_smm_batch_scratch_bytes(stacks, nstacks);
+  int result;
+  if (0 == nbytes) { /* too many parts for one launch set: split the list */
+    const int half = nstacks / 2;
+    if (1 >= nstacks) return EXIT_FAILURE;
+    result = xs_process_batch_part(stacks, half, stream);
+    if (EXIT_SUCCESS == result) result = xs_process_batch_part(stacks + half, nstacks - half, stream);
+    return result;
+  }
+  result = xs_scratch_alloc(&scratch, nbytes, stream);
+  if (EXIT_SUCCESS == result) {
+    result = xs_record_error(xs_launch_smm_batch(stacks, nstacks, scratch, nbytes, stream), "libxstream_b200_process_batch");
+    if (EXIT_SUCCESS != xs_scratch_free(scratch, stream)) result = EXIT_FAILURE;
+  }
+  return result;
+}
+
+int libxstream_b200_process_batch(const libxstream_b200_stack_t* stacks, int nstacks, int max_kernel_dim, void* stream) {
+  int i, nonempty = 0, result;
+  if (0 >= nstacks) return EXIT_SUCCESS;
+  if (NULL == stacks) return EXIT_FAILURE;
+  for (i = 0; i < nstacks; ++i) {
+    const libxstream_b200_stack_t* const d = stacks + i;
+    if (0 > d->stack_size) return -1;
+    if (0 == d->stack_size) continue;
+    if (!libxstream_b200_process_suitable(1, dbcsr_type_real_8, d->stack_size, d->m, d->n, d->k, max_kernel_dim)) return -1;
+    if (NULL == d->dev_param_stack || NULL == d->a || NULL == d->b || NULL == d->c) return EXIT_FAILURE;
+    ++nonempty;
+  }
+  if (0 == nonempty) return EXIT_SUCCESS;
+  result = xs_lazy_init();
+  if (EXIT_SUCCESS != result) return result;
+  return xs_process_batch_part(stacks, nstacks, NULL != stream ? stream : xs_default_stream());
+}
+
 int libxstream_b200_last_error(void) { return xs_last_error(); }
 
 double libxstream_b200_fp64_peak(void* stream) {

@@ -24,8 +24,10 @@
  *   The result is bitwise reproducible from run to run, unlike FP atomics.
  */
 #include "internal.h"
+#include "../../include/libxstream_b200.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 namespace {
 
@@ -95,19 +97,51 @@ __host__ __device__ constexpr int smm_min_blocks(int mt, int nt) { return (mt * 
    a segment that ends inside the chunk is written back at once; pieces of segments crossing chunk
    boundaries are merged inside the CTA through shared memory in warp order, and only segments that
    cross the CTA's own boundaries leave a CTA-level piece in global scratch for the combine kernel. */
+/* What the stack kernel needs to know about one stack: one task for a single call, one per stack
+   for a batch. keys/vals are the stack's grouped entries, pieces its CTA-level piece slots. */
+struct StackTask {
+  const double* a;
+  const double* b;
+  double* c;
+  const unsigned* keys;
+  const unsigned long long* vals;
+  double* pieces;
+  int S, m, n, k;
+  int L, nchunks, ngroups, nsub_n, nsub;
+  int item_begin; /* first work item of this stack (batch) */
+  int cls;        /* tile class (MT - 1) * 4 + (NT - 1) (batch) */
+  int sid;        /* stack index within the call: tag of its segment-list entries */
+};
+
+/* Segment-list entry: stack index (high 8 bits) and CTA group (low 24 bits). */
+__device__ __forceinline__ int seg_tag(int sid, int group) { return (sid << 24) | group; }
+
+/* One work item of the stack kernel: CTA group `group` (W = blockDim.x / 32 consecutive chunks of
+   L grouped entries) and warp sub-tile `sub` of C (8*MT x 8*NT) of one stack. M_, N_, K_ > 0 make
+   the block shape a compile-time constant (every fragment load is then one load at an immediate
+   offset from a per-lane base pointer); 0 means runtime. Per warp: DMMA fragments of the next
+   k-panel (KP k-steps of 4) are loaded while the current panel runs, the A/B blocks two entries ahead
+   are prefetched into L2, and the C sub-tile stays in registers for a whole segment (run of equal
+   c); a segment that ends inside the chunk is written back at once. Pieces of segments crossing
+   chunk boundaries are merged inside the CTA through shared memory in warp order; only segments that
+   cross the CTA's own boundaries leave a CTA-level piece in global scratch for the combine kernel.
+   Ends with a CTA barrier, so shared memory can be reused for the next item. */
 template <int M_, int N_, int K_, int MT, int NT, int KP>
-__global__ void __launch_bounds__(128, smm_min_blocks(MT, NT)) xs_smm_dmma_kernel(const unsigned* __restrict__ keys,
-  const unsigned long long* __restrict__ vals, int S, const double* __restrict__ A, const double* __restrict__ B,
-  double* __restrict__ C, int m_rt, int n_rt, int k_rt, int L, int nchunks, int nsub_n, int nsub,
-  double* __restrict__ pieces, int* __restrict__ seglist) {
+__device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub, int* __restrict__ seglist,
+  double* __restrict__ smem) {
   constexpr int REGS = MT * NT * 2;
-  const int m = M_ ? M_ : m_rt, n = N_ ? N_ : n_rt, k = K_ ? K_ : k_rt;
-  extern __shared__ double smem[];
+  const int m = M_ ? M_ : tk.m, n = N_ ? N_ : tk.n, k = K_ ? K_ : tk.k;
+  const double* __restrict__ const A = tk.a;
+  const double* __restrict__ const B = tk.b;
+  double* __restrict__ const C = tk.c;
+  const unsigned* __restrict__ const keys = tk.keys;
+  const unsigned long long* __restrict__ const vals = tk.vals;
+  const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub_n = tk.nsub_n, nsub = tk.nsub;
+  double* __restrict__ const pieces = tk.pieces;
   const int W = blockDim.x >> 5;
   double* const sp = smem;                                       /* [W][2][REGS][32] */
   int* const meta = (int*)(smem + (size_t)W * 2 * REGS * 32);    /* [W][4]: head, head_spans, tail, spare */
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-  const int group = blockIdx.x / nsub, sub = blockIdx.x - group * nsub;
   const int chunk = group * W + warp;
   const int KS = (k + 3) >> 2;
   const int npan = (KS + KP - 1) / KP;
@@ -262,7 +296,7 @@ __global__ void __launch_bounds__(128, smm_min_blocks(MT, NT)) xs_smm_dmma_kerne
       for (int r = 0; r < REGS; ++r) dst[r * 32] = sum[r];
       if (!from_head && 0 == sub && 0 == lane) {
         const int slotidx = atomicAdd(seglist, 1);
-        seglist[1 + slotidx] = group;
+        seglist[1 + slotidx] = seg_tag(tk.sid, group);
       }
     }
     else {
@@ -279,83 +313,208 @@ __global__ void __launch_bounds__(128, smm_min_blocks(MT, NT)) xs_smm_dmma_kerne
       commit_tile<MT, NT>(C, (size_t)key - 1, tile, m, n, g, t, tl);
     }
   }
+  __syncthreads();
 }
 
-/* Sum the pieces of every chunk-crossing segment in a fixed order and write the block once.
-   One CTA per (segment, sub-tile): its threads first find the segment's last chunk in one parallel
-   probe of chunk-start keys, then its warps sum the pieces round-robin (warp w takes pieces w,
-   w+CW, ...) and warp 0 adds the warp partials in warp order: the summation tree depends only on
-   the number of pieces, so the result is deterministic. */
+template <int M_, int N_, int K_, int MT, int NT, int KP>
+__global__ void __launch_bounds__(128, smm_min_blocks(MT, NT))
+  xs_smm_dmma_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, const unsigned* __restrict__ err) {
+  extern __shared__ double smem[];
+  if (0 != *(volatile const unsigned*)err) return; /* the grouping failed: write nothing */
+  const int group = blockIdx.x / tk.nsub, sub = blockIdx.x - group * tk.nsub;
+  smm_item<M_, N_, K_, MT, NT, KP>(tk, group, sub, seglist, smem);
+}
+
+/* Task table of a batch (kernel parameter: read through the constant bank). */
+constexpr int kMaxBatchTasks = 32;
+struct BatchTasks {
+  int ntasks, nitems;
+  StackTask t[kMaxBatchTasks];
+};
+
+/* One tile class of the batch kernel as a separate (not inlined) function, so that each class gets
+   its own register allocation instead of sharing one with the other classes' code. The largest
+   tiles keep one k-step per register panel: their accumulators alone take 48-64 registers. */
 template <int MT, int NT>
-__global__ void __launch_bounds__(32 * kCombineWarps) xs_smm_combine_kernel(const unsigned* __restrict__ keys, int S,
-  int L, int nchunks, int nsub, int nsub_n, const double* __restrict__ pieces, const int* __restrict__ seglist,
-  double* __restrict__ C, int m, int n) {
+__device__ __noinline__ void batch_item(const StackTask& tk, int group, int sub, int* seglist, double* smem) {
+  smm_item<0, 0, 0, MT, NT, (MT * NT >= 12) ? 1 : 2>(tk, group, sub, seglist, smem);
+}
+
+template <int X, int MT, int NT>
+__device__ __forceinline__ void batch_dispatch(int cls, const StackTask& tk, int group, int sub, int* seglist, double* smem) {
+  if constexpr (MT <= X && NT <= X) {
+    if ((MT - 1) * 4 + (NT - 1) == cls) batch_item<MT, NT>(tk, group, sub, seglist, smem);
+  }
+}
+
+/* Persistent batch kernel: one launch for all stacks of a multiplication. The grid is the number of
+   CTAs resident on the device; each CTA takes work items (CTA group x sub-tile of one stack) from a
+   global queue, in the order the host sorted them (heaviest items first), and runs them with the
+   tile class of their stack (any MT, NT <= X). */
+template <int X>
+__global__ void __launch_bounds__(128, smm_min_blocks(X, X))
+  xs_smm_batch_kernel(const __grid_constant__ BatchTasks bt, int* __restrict__ seglist, unsigned* __restrict__ queue,
+    const unsigned* __restrict__ err) {
+  extern __shared__ double smem[];
+  __shared__ int s_item;
+  if (0 != *(volatile const unsigned*)err) return;
+  for (;;) {
+    if (0 == threadIdx.x) s_item = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= bt.nitems) break;
+    int ti = 0;
+    while (ti + 1 < bt.ntasks && bt.t[ti + 1].item_begin <= item) ++ti;
+    const StackTask& tk = bt.t[ti];
+    const int local = item - tk.item_begin, group = local / tk.nsub, sub = local - group * tk.nsub;
+    const int cls = tk.cls;
+    batch_dispatch<X, 1, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 1, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 1, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 1, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 2, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 2, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 2, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 2, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 3, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 3, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 3, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 3, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 4, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 4, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 4, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<X, 4, 4>(cls, tk, group, sub, seglist, smem);
+  }
+}
+
+/* Sum the pieces of one CTA-crossing segment for one sub-tile in a fixed order and write the block
+   once. The segment starts in CTA group j0 (its tail piece) and continues through the head pieces of
+   the following groups while their first entry still belongs to it; all threads of the CTA find that
+   count in one parallel probe of group-start keys, then its warps sum the pieces round-robin (warp w
+   takes pieces w, w+CW, ...) and warp 0 adds the warp partials in warp order: the summation tree
+   depends only on the number of pieces, so the result is deterministic. */
+template <int MT, int NT>
+__device__ __forceinline__ void combine_one(const StackTask& tk, int W, int j0, int sub, double* __restrict__ red) {
   constexpr int REGS = MT * NT * 2;
   constexpr int CW = kCombineWarps;
-  extern __shared__ double red[]; /* [CW - 1][REGS][32] */
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const unsigned* __restrict__ const keys = tk.keys;
+  const double* __restrict__ const pieces = tk.pieces;
+  const int S = tk.S, Lc = tk.L * W, ngroups = tk.ngroups, nsub = tk.nsub;
+  const unsigned xkey = keys[min((j0 + 1) * Lc, S) - 1];
+  /* pieces = 1 + number of following groups that start inside the segment (a prefix, keys sorted) */
+  int np = 1;
+  for (int base = j0 + 1;; base += blockDim.x) {
+    const int j = base + (int)threadIdx.x;
+    const int inside = (j < ngroups) && (keys[(size_t)j * Lc] == xkey);
+    const int cnt = __syncthreads_count(inside);
+    np += cnt;
+    if (cnt < (int)blockDim.x) break;
+  }
+  double acc[REGS];
+#pragma unroll
+  for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
+  int q = warp;
+  for (; q + CW < np; q += 2 * CW) { /* two pieces in flight per step */
+    const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q), s1 = 2 * (j0 + q + CW);
+    const double* const p0 = pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
+    const double* const p1 = pieces + ((size_t)s1 * nsub + sub) * REGS * 32 + lane;
+    double v0[REGS], v1[REGS];
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) {
+      v0[r] = p0[r * 32];
+      v1[r] = p1[r * 32];
+    }
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] += v0[r];
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] += v1[r];
+  }
+  if (q < np) {
+    const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q);
+    const double* const p0 = pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] += p0[r * 32];
+  }
+  if (0 != warp) {
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) red[((warp - 1) * REGS + r) * 32 + lane] = acc[r];
+  }
+  __syncthreads();
+  if (0 == warp) {
+    for (int w2 = 0; w2 < CW - 1; ++w2) {
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += red[(w2 * REGS + r) * 32 + lane];
+    }
+    Tile<MT, NT> tl;
+    tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
+    double tile[MT][NT][2];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        tile[i][j][0] = acc[(i * NT + j) * 2 + 0];
+        tile[i][j][1] = acc[(i * NT + j) * 2 + 1];
+      }
+    commit_tile<MT, NT>(tk.c, (size_t)xkey - 1, tile, tk.m, tk.n, g, t, tl);
+  }
+  __syncthreads();
+}
+
+/* Combine of a single stack: grid-stride over (segment-list entry, sub-tile). */
+template <int MT, int NT>
+__global__ void __launch_bounds__(32 * kCombineWarps)
+  xs_smm_combine_kernel(const __grid_constant__ StackTask tk, int W, const int* __restrict__ seglist,
+    const unsigned* __restrict__ err) {
+  extern __shared__ double red[]; /* [CW - 1][REGS][32] */
+  if (0 != *(volatile const unsigned*)err) return;
   const int count = seglist[0];
-  for (int w = blockIdx.x; w < count * nsub; w += gridDim.x) {
-    const int li = w / nsub, sub = w - li * nsub;
-    const int j0 = seglist[1 + li];
-    const unsigned xkey = keys[min((j0 + 1) * L, S) - 1];
-    /* pieces = 1 + number of following chunks that start inside the segment (a prefix, keys sorted) */
-    int np = 1;
-    for (int base = j0 + 1;; base += blockDim.x) {
-      const int j = base + (int)threadIdx.x;
-      const int inside = (j < nchunks) && (keys[(size_t)j * L] == xkey);
-      const int cnt = __syncthreads_count(inside);
-      np += cnt;
-      if (cnt < (int)blockDim.x) break;
+  for (int w = blockIdx.x; w < count * tk.nsub; w += gridDim.x) {
+    const int li = w / tk.nsub, sub = w - li * tk.nsub;
+    combine_one<MT, NT>(tk, W, seglist[1 + li] & 0xFFFFFF, sub, red);
+  }
+}
+
+template <int X, int MT, int NT>
+__device__ __forceinline__ void combine_dispatch(int cls, const StackTask& tk, int W, int j0, int sub, double* red) {
+  if constexpr (MT <= X && NT <= X) {
+    if ((MT - 1) * 4 + (NT - 1) == cls) combine_one<MT, NT>(tk, W, j0, sub, red);
+  }
+}
+
+/* Combine of a batch: grid-stride over segment-list entries; each entry names its stack. */
+template <int X>
+__global__ void __launch_bounds__(32 * kCombineWarps)
+  xs_smm_combine_batch_kernel(const __grid_constant__ BatchTasks bt, int W, const int* __restrict__ seglist,
+    const unsigned* __restrict__ err) {
+  extern __shared__ double red[];
+  if (0 != *(volatile const unsigned*)err) return;
+  const int count = seglist[0];
+  for (int li = blockIdx.x; li < count; li += gridDim.x) {
+    const int tag = seglist[1 + li], sid = tag >> 24, j0 = tag & 0xFFFFFF;
+    int ti = 0;
+    while (ti + 1 < bt.ntasks && bt.t[ti].sid != sid) ++ti;
+    const StackTask& tk = bt.t[ti];
+    for (int sub = 0; sub < tk.nsub; ++sub) {
+      const int cls = tk.cls;
+      combine_dispatch<X, 1, 1>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 1, 2>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 1, 3>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 1, 4>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 2, 1>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 2, 2>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 2, 3>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 2, 4>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 3, 1>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 3, 2>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 3, 3>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 3, 4>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 4, 1>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 4, 2>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 4, 3>(cls, tk, W, j0, sub, red);
+      combine_dispatch<X, 4, 4>(cls, tk, W, j0, sub, red);
     }
-    double acc[REGS];
-#pragma unroll
-    for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
-    int q = warp;
-    for (; q + CW < np; q += 2 * CW) { /* two pieces in flight per step */
-      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q), s1 = 2 * (j0 + q + CW);
-      const double* const p0 = pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
-      const double* const p1 = pieces + ((size_t)s1 * nsub + sub) * REGS * 32 + lane;
-      double v0[REGS], v1[REGS];
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) {
-        v0[r] = p0[r * 32];
-        v1[r] = p1[r * 32];
-      }
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) acc[r] += v0[r];
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) acc[r] += v1[r];
-    }
-    if (q < np) {
-      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q);
-      const double* const p0 = pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) acc[r] += p0[r * 32];
-    }
-    if (0 != warp) {
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) red[((warp - 1) * REGS + r) * 32 + lane] = acc[r];
-    }
-    __syncthreads();
-    if (0 == warp) {
-      for (int w2 = 0; w2 < CW - 1; ++w2) {
-#pragma unroll
-        for (int r = 0; r < REGS; ++r) acc[r] += red[(w2 * REGS + r) * 32 + lane];
-      }
-      Tile<MT, NT> tl;
-      tl.init(sub, nsub_n, m, n, g);
-      double tile[MT][NT][2];
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-          tile[i][j][0] = acc[(i * NT + j) * 2 + 0];
-          tile[i][j][1] = acc[(i * NT + j) * 2 + 1];
-        }
-      commit_tile<MT, NT>(C, (size_t)xkey - 1, tile, m, n, g, t, tl);
-    }
-    __syncthreads();
   }
 }
 
@@ -367,8 +526,10 @@ struct SmmPlan {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-typedef cudaError_t (*launch_fn_t)(const SmmPlan&, const unsigned*, const unsigned long long*, int, const double*,
-  const double*, double*, int, int, int, double*, int*, cudaStream_t, int*);
+/* Launches the stack and combine kernels of one stack; with occ != nullptr it only reports how many
+   CTAs of W = pl.W warps fit on one SM (the plan sizes chunks from that). */
+typedef cudaError_t (*launch_fn_t)(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err,
+  cudaStream_t s, int* occ);
 
 launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm);
 
@@ -384,11 +545,9 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   if (0 < prm->chunk) pl->L = prm->chunk;
   else {
     int occ = 0;
+    StackTask none = {};
     const launch_fn_t fn = find_launcher(m, n, k, prm);
-    if (cudaSuccess != fn(*pl, nullptr, nullptr, 0, nullptr, nullptr, nullptr, m, n, k, nullptr, nullptr, 0, &occ) ||
-        occ < 1) {
-      occ = 1;
-    }
+    if (cudaSuccess != fn(*pl, none, nullptr, nullptr, 0, &occ) || occ < 1) occ = 1;
     const long resident = (long)occ * xs_sm_count();
     const long L = ((long)S * pl->nsub + resident * pl->W - 1) / (resident * pl->W);
     pl->L = (int)(L < 1 ? 1 : L);
@@ -410,7 +569,7 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   pl->off_vals_out = off;
   off += vs;
   pl->off_seglist = off;
-  off = align_up(off + sizeof(int) * ((size_t)pl->nchunks + 1), 256);
+  off = align_up(off + sizeof(int) * ((size_t)pl->ngroups + 1), 256);
   pl->off_pieces = off;
   off = align_up(off + sizeof(double) * (size_t)2 * pl->ngroups * pl->nsub * (mt * nt * 2) * 32, 256);
   pl->off_sort = off;
@@ -419,11 +578,9 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   return 0;
 }
 
-/* Launches the stack kernel and the combine kernel for one planned call. With occ != nullptr it
-   only reports how many CTAs of W = pl.W warps fit on one SM (the plan sizes chunks from that). */
 template <int M_, int N_, int K_, int MT, int NT, int KP>
-cudaError_t launch_dmma(const SmmPlan& pl, const unsigned* keys, const unsigned long long* vals, int S, const double* a,
-  const double* b, double* c, int m, int n, int k, double* pieces, int* seglist, cudaStream_t s, int* occ) {
+cudaError_t launch_dmma(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err, cudaStream_t s,
+  int* occ) {
   cudaError_t r;
   static int smem_set = 0, csmem_set = 0; /* per template instance; setting them twice is harmless */
   const size_t smem = smm_smem_bytes<MT, NT>(pl.W);
@@ -437,11 +594,11 @@ cudaError_t launch_dmma(const SmmPlan& pl, const unsigned* keys, const unsigned 
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, 32 * pl.W, smem);
   }
   void* prof = xs_profile_begin(s);
-  xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP><<<pl.ngroups * pl.nsub, 32 * pl.W, smem, s>>>(
-    keys, vals, S, a, b, c, m, n, k, pl.L, pl.nchunks, pl.nsub_n, pl.nsub, pieces, seglist);
+  xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP><<<pl.ngroups * pl.nsub, 32 * pl.W, smem, s>>>(tk, seglist, err);
   r = cudaGetLastError();
   if (cudaSuccess != r) return r;
-  xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)S, 8.0 * S * ((double)m * k + (double)k * n + 2.0 * m * n), s);
+  const double m = tk.m, n = tk.n, k = tk.k;
+  xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
   const int cgrid = max(1, min(pl.ngroups * pl.nsub, 2 * xs_sm_count()));
   const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (MT * NT * 2) * 32;
   if (!csmem_set) {
@@ -450,9 +607,7 @@ cudaError_t launch_dmma(const SmmPlan& pl, const unsigned* keys, const unsigned 
     csmem_set = 1;
   }
   prof = xs_profile_begin(s);
-  /* the combine works on CTA ranges: W*L entries per "chunk", one range per CTA group */
-  xs_smm_combine_kernel<MT, NT><<<cgrid, 32 * kCombineWarps, csmem, s>>>(
-    keys, S, pl.L * pl.W, pl.ngroups, pl.nsub, pl.nsub_n, pieces, seglist, c, m, n);
+  xs_smm_combine_kernel<MT, NT><<<cgrid, 32 * kCombineWarps, csmem, s>>>(tk, pl.W, seglist, err);
   r = cudaGetLastError();
   xs_profile_end(prof, "combine", 0.0, 0.0, s);
   return r;
@@ -487,6 +642,188 @@ launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
     }
   }
   return launch_table[prm->mt - 1][prm->nt - 1][(4 == prm->kp) ? 1 : 0];
+}
+
+/* ------------------------------------------------------------------- batch of stacks (one launch) */
+
+constexpr int kBatchW = 4; /* warps per CTA of the batch kernel */
+
+size_t batch_smem_bytes(int X) { return (size_t)kBatchW * (2 * X * X * 2 * 32 * sizeof(double) + 4 * sizeof(int)); }
+
+template <int X>
+cudaError_t batch_prepare(int* occ) {
+  static int done = 0, occ_cached = 0;
+  cudaError_t r = cudaSuccess;
+  if (!done) {
+    const size_t smem = batch_smem_bytes(X);
+    const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32;
+    if (smem > 48 * 1024) r = cudaFuncSetAttribute(xs_smm_batch_kernel<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaSuccess == r && csmem > 48 * 1024) {
+      r = cudaFuncSetAttribute(xs_smm_combine_batch_kernel<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+    }
+    if (cudaSuccess == r) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_cached, xs_smm_batch_kernel<X>, 32 * kBatchW, smem);
+    if (cudaSuccess != r) return r;
+    done = 1;
+  }
+  if (nullptr != occ) *occ = occ_cached;
+  return r;
+}
+
+cudaError_t batch_occupancy(int X, int* occ) {
+  switch (X) {
+    case 1: return batch_prepare<1>(occ);
+    case 2: return batch_prepare<2>(occ);
+    case 3: return batch_prepare<3>(occ);
+    default: return batch_prepare<4>(occ);
+  }
+}
+
+template <int X>
+cudaError_t batch_run(const BatchTasks& bt, int ngroups_total, int* seglist, unsigned* queue, const unsigned* err,
+  double flops, double bytes, cudaStream_t s) {
+  int occ = 0;
+  cudaError_t r = batch_prepare<X>(&occ);
+  if (cudaSuccess != r) return r;
+  const int grid = max(1, min(bt.nitems, max(1, occ) * xs_sm_count()));
+  void* prof = xs_profile_begin(s);
+  xs_smm_batch_kernel<X><<<grid, 32 * kBatchW, batch_smem_bytes(X), s>>>(bt, seglist, queue, err);
+  r = cudaGetLastError();
+  if (cudaSuccess != r) return r;
+  xs_profile_end(prof, "smm_batch", flops, bytes, s);
+  prof = xs_profile_begin(s);
+  const int cgrid = max(1, min(ngroups_total, 2 * xs_sm_count()));
+  xs_smm_combine_batch_kernel<X><<<cgrid, 32 * kCombineWarps, sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32, s>>>(
+    bt, kBatchW, seglist, err);
+  r = cudaGetLastError();
+  xs_profile_end(prof, "combine_batch", 0.0, 0.0, s);
+  return r;
+}
+
+/* One part of a batch: a stack, or a slice of a stack larger than one grouping launch takes. */
+struct BatchPart {
+  int stack; /* index into the caller's array */
+  int first; /* first entry of the slice */
+  int S;
+  int mt, nt;
+  double item_cost;
+};
+
+struct BatchPlan {
+  int nparts, X, ntotal, ngroups_total, nitems;
+  BatchPart part[kMaxBatchTasks];
+  int L[kMaxBatchTasks], nsub[kMaxBatchTasks], nsub_n[kMaxBatchTasks], ngroups[kMaxBatchTasks];
+  size_t off_part[kMaxBatchTasks], pieces_off[kMaxBatchTasks];
+  int order[kMaxBatchTasks]; /* parts by descending item cost */
+  size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces, off_sort;
+  size_t total;
+};
+
+int pick_tiles_dim(int dim) { /* least padded split of ceil(dim/8) fragments into sub-tiles of <= 4 */
+  const int frags = (dim + 7) / 8;
+  int best = 1, bestwaste = 1 << 30;
+  for (int t = 4; t >= 1; --t) {
+    const int waste = (frags + t - 1) / t * t - frags;
+    if (waste < bestwaste) {
+      bestwaste = waste;
+      best = t;
+    }
+  }
+  return best;
+}
+
+/* Work decomposition of a batch: stacks split into parts of at most xs_stack_group_max() entries;
+   per part a tile class (MT x NT from the parameter table) and a chunk length L chosen so that every
+   work item (W chunks x one sub-tile) costs about the same, ~4 items per resident CTA. */
+int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
+  const int smax = xs_stack_group_max();
+  bp->nparts = 0;
+  bp->X = 1;
+  bp->ntotal = 0;
+  for (int i = 0; i < ns; ++i) {
+    if (0 >= st[i].stack_size) continue;
+    xs_smm_params_t prm;
+    xs_params_lookup(3, st[i].m, st[i].n, st[i].k, st[i].stack_size, &prm);
+    for (int first = 0; first < st[i].stack_size; first += smax) {
+      if (bp->nparts == kMaxBatchTasks) return -1;
+      BatchPart& p = bp->part[bp->nparts++];
+      p.stack = i;
+      p.first = first;
+      p.S = min(smax, st[i].stack_size - first);
+      p.mt = prm.mt;
+      p.nt = prm.nt;
+      if (p.mt > bp->X) bp->X = p.mt;
+      if (p.nt > bp->X) bp->X = p.nt;
+      bp->ntotal += p.S;
+    }
+  }
+  if (0 == bp->nparts) return 0;
+  int occ = 0;
+  if (cudaSuccess != batch_occupancy(bp->X, &occ) || occ < 1) occ = 1;
+  /* cost units: DMMA instructions per entry per warp plus a fixed per-entry overhead */
+  double total = 0;
+  for (int q = 0; q < bp->nparts; ++q) {
+    const BatchPart& p = bp->part[q];
+    const libxstream_b200_stack_t& d = st[p.stack];
+    const int nsub = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
+    total += (double)p.S * nsub * (p.mt * p.nt * ((d.k + 3) / 4) + 8);
+  }
+  const double target = total / ((double)occ * xs_sm_count() * 4.0); /* cost of one work item */
+  size_t off = 0, poff = 0;
+  bp->ngroups_total = 0;
+  bp->nitems = 0;
+  for (int q = 0; q < bp->nparts; ++q) {
+    BatchPart& p = bp->part[q];
+    const libxstream_b200_stack_t& d = st[p.stack];
+    bp->nsub_n[q] = (((d.n + 7) / 8) + p.nt - 1) / p.nt;
+    bp->nsub[q] = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * bp->nsub_n[q];
+    const double per_entry = p.mt * p.nt * ((d.k + 3) / 4) + 8;
+    long L = (long)(target / (kBatchW * per_entry) + 0.5);
+    if (L < 1) L = 1;
+    if (L > p.S) L = p.S;
+    bp->L[q] = (int)L;
+    const int nchunks = (int)((p.S + L - 1) / L);
+    bp->ngroups[q] = (nchunks + kBatchW - 1) / kBatchW;
+    p.item_cost = (double)kBatchW * L * per_entry;
+    bp->off_part[q] = off;
+    off += (size_t)p.S;
+    bp->pieces_off[q] = poff;
+    poff += (size_t)2 * bp->ngroups[q] * bp->nsub[q] * (p.mt * p.nt * 2) * 32;
+    bp->ngroups_total += bp->ngroups[q];
+    bp->nitems += bp->ngroups[q] * bp->nsub[q];
+    bp->order[q] = q;
+  }
+  for (int a = 1; a < bp->nparts; ++a) { /* heaviest items first (insertion sort, stable) */
+    const int v = bp->order[a];
+    int b = a - 1;
+    while (b >= 0 && bp->part[bp->order[b]].item_cost < bp->part[v].item_cost) {
+      bp->order[b + 1] = bp->order[b];
+      --b;
+    }
+    bp->order[b + 1] = v;
+  }
+  const size_t N = (size_t)bp->ntotal;
+  size_t o = 0;
+  const size_t ks = align_up(sizeof(unsigned) * N, 256), vs = align_up(sizeof(unsigned long long) * N, 256);
+  bp->off_keys_in = o;
+  o += ks;
+  bp->off_keys_tmp = o;
+  o += ks;
+  bp->off_keys_out = o;
+  o += ks;
+  bp->off_vals_in = o;
+  o += vs;
+  bp->off_vals_tmp = o;
+  o += vs;
+  bp->off_vals_out = o;
+  o += vs;
+  bp->off_seglist = o;
+  o = align_up(o + sizeof(int) * ((size_t)bp->ngroups_total + 1), 256);
+  bp->off_pieces = o;
+  o = align_up(o + sizeof(double) * poff, 256);
+  bp->off_sort = o;
+  o = align_up(o + xs_sort_ctl_bytes() + sizeof(int) * ((size_t)xs_sort_launch_tiles() + XS_MAX_BATCH) * 2048, 256);
+  bp->total = o;
+  return bp->nparts;
 }
 
 /* ------------------------------------------------------------------------------ transpose */
@@ -592,17 +929,124 @@ int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double
   unsigned long long* const vals_tmp = (unsigned long long*)(base + pl.off_vals_tmp);
   unsigned long long* const vals_out = (unsigned long long*)(base + pl.off_vals_out);
   int* const seglist = (int*)(base + pl.off_seglist);
-  double* const pieces = (double*)(base + pl.off_pieces);
   void* const sort_scratch = base + pl.off_sort;
   void* prof = xs_profile_begin(s);
   const int r = xs_stack_group(dev_stack, S, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, seglist,
     sort_scratch, s);
   if (0 != r) return r;
   xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
-  const unsigned* const keys = keys_out;
-  const unsigned long long* const vals = vals_out;
+  StackTask tk = {};
+  tk.a = a;
+  tk.b = b;
+  tk.c = c;
+  tk.keys = keys_out;
+  tk.vals = vals_out;
+  tk.pieces = (double*)(base + pl.off_pieces);
+  tk.S = S;
+  tk.m = m;
+  tk.n = n;
+  tk.k = k;
+  tk.L = pl.L;
+  tk.nchunks = pl.nchunks;
+  tk.ngroups = pl.ngroups;
+  tk.nsub_n = pl.nsub_n;
+  tk.nsub = pl.nsub;
   const launch_fn_t fn = find_launcher(m, n, k, prm);
-  return (int)fn(pl, keys, vals, S, a, b, c, m, n, k, pieces, seglist, s, nullptr);
+  return (int)fn(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
+}
+
+size_t xs_smm_batch_scratch_bytes(const libxstream_b200_stack_t* stacks, int nstacks) {
+  BatchPlan bp;
+  if (0 >= plan_batch(stacks, nstacks, &bp)) return 0;
+  return bp.total;
+}
+
+int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch, size_t scratch_bytes, void* stream) {
+  BatchPlan bp;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int np = plan_batch(st, ns, &bp);
+  if (0 > np) return (int)cudaErrorInvalidValue;
+  if (0 == np) return 0;
+  if (scratch_bytes < bp.total || nullptr == scratch) return (int)cudaErrorInvalidValue;
+  char* const base = (char*)scratch;
+  unsigned* const k0 = (unsigned*)(base + bp.off_keys_in);
+  unsigned* const k1 = (unsigned*)(base + bp.off_keys_tmp);
+  unsigned* const kout = (unsigned*)(base + bp.off_keys_out);
+  unsigned long long* const v0 = (unsigned long long*)(base + bp.off_vals_in);
+  unsigned long long* const v1 = (unsigned long long*)(base + bp.off_vals_tmp);
+  unsigned long long* const vout = (unsigned long long*)(base + bp.off_vals_out);
+  int* const seglist = (int*)(base + bp.off_seglist);
+  double* const pieces = (double*)(base + bp.off_pieces);
+  void* const sort_scratch = base + bp.off_sort;
+  /* grouping: one control block for the call, then as few grouping launches as the tiles need */
+  int r = xs_sort_clear_ctl(sort_scratch, bp.nparts, s);
+  if (0 != r) return r;
+  void* prof = xs_profile_begin(s);
+  xs_sort_batch_t sb;
+  sb.nstacks = 0;
+  int tiles = 0;
+  const int launch_tiles = xs_sort_launch_tiles(), tile_entries = xs_sort_tile_entries(1);
+  for (int q = 0; q <= bp.nparts; ++q) {
+    const int nt = (q < bp.nparts) ? (bp.part[q].S + tile_entries - 1) / tile_entries : 0;
+    if (q == bp.nparts || sb.nstacks == XS_MAX_BATCH || tiles + nt > launch_tiles) {
+      if (0 < sb.nstacks) {
+        r = xs_stack_group_batch(&sb, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, s);
+        if (0 != r) return r;
+      }
+      sb.nstacks = 0;
+      tiles = 0;
+    }
+    if (q == bp.nparts) break;
+    const BatchPart& p = bp.part[q];
+    sb.gidx[sb.nstacks] = q;
+    sb.stack[sb.nstacks] = st[p.stack].dev_param_stack + 3 * (size_t)p.first;
+    sb.S[sb.nstacks] = p.S;
+    sb.off[sb.nstacks] = (int)bp.off_part[q];
+    ++sb.nstacks;
+    tiles += nt;
+  }
+  xs_profile_end(prof, "sort", 0.0, 48.0 * bp.ntotal, s);
+  BatchTasks bt;
+  memset(&bt, 0, sizeof(bt));
+  bt.ntasks = bp.nparts;
+  bt.nitems = bp.nitems;
+  double flops = 0, bytes = 0;
+  int item = 0;
+  for (int i = 0; i < bp.nparts; ++i) {
+    const int q = bp.order[i];
+    const BatchPart& p = bp.part[q];
+    const libxstream_b200_stack_t& d = st[p.stack];
+    StackTask& tk = bt.t[i];
+    tk.a = (const double*)d.a;
+    tk.b = (const double*)d.b;
+    tk.c = (double*)d.c;
+    tk.keys = kout + bp.off_part[q];
+    tk.vals = vout + bp.off_part[q];
+    tk.pieces = pieces + bp.pieces_off[q];
+    tk.S = p.S;
+    tk.m = d.m;
+    tk.n = d.n;
+    tk.k = d.k;
+    tk.L = bp.L[q];
+    tk.nchunks = (p.S + bp.L[q] - 1) / bp.L[q];
+    tk.ngroups = bp.ngroups[q];
+    tk.nsub_n = bp.nsub_n[q];
+    tk.nsub = bp.nsub[q];
+    tk.item_begin = item;
+    tk.cls = (p.mt - 1) * 4 + (p.nt - 1);
+    tk.sid = q;
+    item += tk.ngroups * tk.nsub;
+    flops += 2.0 * d.m * d.n * d.k * (double)p.S;
+    bytes += 8.0 * p.S * ((double)d.m * d.k + (double)d.k * d.n + 2.0 * d.m * d.n);
+  }
+  unsigned* const queue = xs_sort_queue_counter(sort_scratch);
+  const unsigned* const err = xs_sort_error_flag(sort_scratch);
+  switch (bp.X) {
+    case 1: return (int)batch_run<1>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
+    case 2: return (int)batch_run<2>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
+    case 3: return (int)batch_run<3>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
+    default: return (int)batch_run<4>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
+  }
 }
 
 int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize, int m, int n, void* stream) {

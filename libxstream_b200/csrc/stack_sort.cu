@@ -1,21 +1,26 @@
 /*
- * Stable device sort of a stack by its c offset (the grouping step of the plain FP64 stack path).
+ * Stable device grouping of stacks by their c offset (the first step of the plain FP64 stack path),
+ * for one stack or a batch of stacks in one cooperative kernel.
  *
  * The c offsets of one stack are few distinct values spread over a large range (C blocks of one
- * shape in a pool), so they are first mapped to dense bucket ids id = (c - cmin) / g, where g is the
- * gcd of all differences c - c0 (for a pool of equal blocks g is the block size). The extract kernel
- * one cooperative kernel computes cmin, cmax and g (phase 0, while it splits the stack into keys
- * and payload) and then runs an LSD counting sort over the ids with digits of at most 2048
- * buckets: a single pass when the stack touches at most 2048 distinct C blocks (the common case),
- * two or three otherwise. Per pass: per-tile digit histograms -> one exclusive scan per digit over the tiles ->
- * stable scatter (rank within a tile from warp match masks and per-warp counts). The ordering of
- * equal keys is the stack order, so the permutation is bit-exact and reproducible.
- * Grid-wide barriers spin on a global counter with an iteration limit; on timeout the kernel sets
- * an error flag and returns, and the host reports the error instead of hanging.
+ * shape in a pool), so they are mapped to dense bucket ids id = (c - cmin) / g, where g is the gcd
+ * of all differences c - c0 (for a pool of equal blocks g is the block size). Phase 0 of the kernel
+ * splits each stack into keys (c) and payload (a | b << 32) and gathers cmin, cmax and g per stack;
+ * then an LSD counting sort over the ids runs with digits of at most 2048 buckets: a single pass when
+ * a stack touches at most 2048 distinct C blocks (the common case), two or three otherwise. Per pass:
+ * per-tile digit histograms -> digit bases -> stable scatter (rank within a tile from warp match
+ * masks and per-warp counts). Every tile belongs to one stack and every stack is sorted inside its
+ * own range of the output; equal keys keep stack order, so the permutation is bit-exact and
+ * reproducible. Grid-wide barriers spin on a global counter with an iteration limit; on timeout the
+ * kernel sets the call's error flag (the stack kernel then writes nothing) and the library's device
+ * error word, and returns instead of hanging.
  */
 #include "internal.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+/* Library-wide device error word: bit 0 = a grid barrier of the grouping sort timed out. */
+__device__ unsigned xs_device_error_word;
 
 namespace {
 
@@ -24,11 +29,14 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kRadixBits = 11;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr unsigned kSpinLimit = 1u << 24;
+constexpr int kMaxGroupTiles = 256; /* the owner-warp digit scan covers at most 256 tiles per stack */
 
-/* Zero-initialised by one memset per call: the minimum is kept as its complement (atomicMax). */
+/* Control block of one call, zero-initialised by one memset at the start of the call:
+   ctl[0] holds the grid barrier, the error flag and the stack kernel's work-queue counter;
+   ctl[1 + g] the statistics of stack g of the call (the minimum kept as its complement, atomicMax). */
 struct SortCtl {
   unsigned ncmin, cmax, gcd, pad0;
-  unsigned bar_count, bar_gen, err, pad1;
+  unsigned bar_count, bar_gen, err, queue;
 };
 
 /* gcd by Stein's binary method (shifts and subtractions, no integer division). */
@@ -47,6 +55,11 @@ __device__ __forceinline__ unsigned gcd_u(unsigned a, unsigned b) {
     b -= a;
   } while (0 != b);
   return a << sh;
+}
+
+/* Extend a running gcd by x; skips the gcd when g already divides x (the common case). */
+__device__ __forceinline__ unsigned gcd_acc(unsigned g, unsigned x) {
+  return (0 != g && 0 == x % g) ? g : gcd_u(g, x);
 }
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -76,6 +89,7 @@ __device__ bool grid_sync(SortCtl* ctl) {
       while (*vgen == gen) {
         if (++spins > kSpinLimit) {
           atomicExch(&ctl->err, 1u);
+          atomicOr(&xs_device_error_word, 1u);
           ok = 0;
           break;
         }
@@ -87,11 +101,6 @@ __device__ bool grid_sync(SortCtl* ctl) {
   }
   __syncthreads();
   return 0 != s_ok;
-}
-
-/* Extend a running gcd by x; skips the gcd when g already divides x (the common case). */
-__device__ __forceinline__ unsigned gcd_acc(unsigned g, unsigned x) {
-  return (0 != g && 0 == x % g) ? g : gcd_u(g, x);
 }
 
 /* Bucket id (c - cmin) / g. g divides every c - cmin, so the quotient is an exact integer below
@@ -126,33 +135,34 @@ __device__ __forceinline__ void block_exscan(int (&v)[PER], int* s_wsum) {
   __syncthreads();
 }
 
-/* Extract + stable LSD counting sort of a stack by bucket id, one cooperative kernel.
-   Layout: CTA = tile of up to kSortThreads*E consecutive entries; warp w owns the contiguous
-   sub-range [w0, w0 + 32E) and lane l holds entries w0 + l + 32r (r < E) in registers for the
-   whole kernel, so every phase costs about one round trip to memory.
-   Phase 0: load the AoS stack, contribute min(c), max(c) and the gcd of c - c0 (one set of atomics
-   per CTA). Per pass (radix R = 2^rb <= 2048 buckets, as few passes as the bucket range needs):
-   tile histograms hist[tile][digit] -> barrier -> digit bases of this tile (exclusive scan over
-   digits of the digit totals plus the prefix over lower tiles; computed directly when the table is
-   small, else by one owner thread per digit and a second barrier) -> stable scatter: each warp
-   counts its digits, the counts become per-warp offsets, each warp places its entries in order
-   (ranks inside 32 entries from match masks). Later passes reload their tile from the previous
-   pass's output after a barrier. */
+/* Grouping sort of a batch of stacks. Tile t belongs to stack s with tile_begin[s] <= t <
+   tile_begin[s] + ntiles[s]; it covers entries [lt*T, min(S_s, (lt+1)*T)) of that stack (lt =
+   t - tile_begin[s], T = kSortThreads*E). Warp w owns the contiguous sub-range [w0, w0 + 32E) of
+   the tile and lane l holds entries w0 + l + 32r (r < E) in registers for the whole kernel, so every
+   phase costs about one round trip to memory. Output positions of stack s are off[s] + local.
+   Histogram table: rows hist[t][0..kRadix) per tile, then one totals row per stack. */
 template <int E>
-__global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int* __restrict__ stack, int S,
-  unsigned* __restrict__ k0, unsigned long long* __restrict__ v0, unsigned* __restrict__ k1,
-  unsigned long long* __restrict__ v1, unsigned* __restrict__ kout, unsigned long long* __restrict__ vout,
-  int* __restrict__ seglist, int* __restrict__ hist, SortCtl* ctl, unsigned long long* __restrict__ stamps) {
+__global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_batch_t desc, unsigned* __restrict__ k0,
+  unsigned long long* __restrict__ v0, unsigned* __restrict__ k1, unsigned long long* __restrict__ v1,
+  unsigned* __restrict__ kout, unsigned long long* __restrict__ vout, int* __restrict__ seglist,
+  int* __restrict__ hist, SortCtl* ctl, unsigned long long* __restrict__ stamps) {
   __shared__ unsigned short s_wc[kSortWarps][kRadix];
   __shared__ int s_base[kRadix]; /* digit histogram in (a), digit write positions in (b)/(c) */
   __shared__ int s_wsum[kSortWarps];
   __shared__ unsigned s_red[3][kSortWarps];
-  const int G = gridDim.x, tile = blockIdx.x;
-  const int T = (S + G - 1) / G, t0 = min(S, tile * T), t1 = min(S, t0 + T);
+  __shared__ int s_radix[XS_MAX_BATCH]; /* digit range R of every stack of the batch */
+  const int tile = blockIdx.x, ntiles_all = gridDim.x;
+  int si = 0;
+  while (si + 1 < desc.nstacks && desc.tile_begin[si + 1] <= tile) ++si;
+  const int* const stack = desc.stack[si];
+  const int S = desc.S[si], off = desc.off[si], tb = desc.tile_begin[si], G = desc.ntiles[si];
+  const int lt = tile - tb, T = kSortThreads * E;
+  const int t0 = min(S, lt * T), t1 = min(S, t0 + T);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w0 = min(t1, t0 + warp * 32 * E), w1 = min(t1, w0 + 32 * E);
   unsigned key[E];
   unsigned long long val[E];
+  SortCtl* const sctl = ctl + 1 + desc.gidx[si];
   /* optional phase timestamps (stamps != nullptr): [tile][8] */
 #define XS_STAMP(slot) \
   do { \
@@ -160,7 +170,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int*
   } while (0)
   XS_STAMP(0);
 
-  /* phase 0: load + bucket statistics */
+  /* phase 0: load + bucket statistics of this stack */
   {
     const unsigned c0 = (unsigned)stack[2];
     unsigned lo = 0xFFFFFFFFu, hi = 0u, gg = 0u;
@@ -203,25 +213,39 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int*
         gg = gcd_acc(gg, s_red[2][w]);
       }
       if (lo != 0xFFFFFFFFu) {
-        atomicMax(&ctl->ncmin, ~lo);
-        atomicMax(&ctl->cmax, hi);
+        atomicMax(&sctl->ncmin, ~lo);
+        atomicMax(&sctl->cmax, hi);
       }
       if (0 != gg) {
-        unsigned old = *(volatile unsigned*)&ctl->gcd;
+        unsigned old = *(volatile unsigned*)&sctl->gcd;
         while (0 == old || gcd_u(old, gg) != old) { /* no CAS once the global gcd divides this one */
           const unsigned assumed = old;
-          old = atomicCAS(&ctl->gcd, assumed, gcd_u(assumed, gg));
+          old = atomicCAS(&sctl->gcd, assumed, gcd_u(assumed, gg));
           if (old == assumed) break;
         }
       }
-      if (0 == tile) seglist[0] = 0;
+      if (0 == tile && nullptr != seglist) seglist[0] = 0;
     }
     XS_STAMP(1);
     if (!grid_sync(ctl)) return;
     XS_STAMP(2);
   }
-  const unsigned cmin = ~*(volatile unsigned*)&ctl->ncmin, g = *(volatile unsigned*)&ctl->gcd;
-  const unsigned cmax = *(volatile unsigned*)&ctl->cmax;
+  /* per-stack digit plan; every CTA derives the same pass count and table mode for the whole batch
+     (the number of grid barriers must be uniform) */
+  int passes_all = 0, rows_max = 0;
+  for (int s2 = 0; s2 < desc.nstacks; ++s2) {
+    const SortCtl* const c2 = ctl + 1 + desc.gidx[s2];
+    const unsigned g2 = *(volatile const unsigned*)&c2->gcd;
+    const unsigned nb2 = (0 == g2) ? 1u : (*(volatile const unsigned*)&c2->cmax - ~*(volatile const unsigned*)&c2->ncmin) / g2 + 1u;
+    int b2 = 0;
+    while (b2 < 32 && (nb2 - 1u) >> b2) ++b2;
+    const int p2 = (b2 + kRadixBits - 1) / kRadixBits;
+    if (0 == threadIdx.x) s_radix[s2] = (0 == p2) ? 1 : 1 << ((b2 + p2 - 1) / p2);
+    if (p2 > passes_all) passes_all = p2;
+    if (desc.ntiles[s2] > rows_max) rows_max = desc.ntiles[s2];
+  }
+  const unsigned cmin = ~*(volatile unsigned*)&sctl->ncmin, g = *(volatile unsigned*)&sctl->gcd;
+  const unsigned cmax = *(volatile unsigned*)&sctl->cmax;
   const unsigned nb = (0 == g) ? 1u : (cmax - cmin) / g + 1u;
   const double inv_g = (0 == g) ? 0.0 : 1.0 / (double)g;
   int bits = 0;
@@ -232,15 +256,15 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int*
     for (int r = 0; r < E; ++r) {
       const int i = w0 + lane + 32 * r;
       if (i < w1) {
-        kout[i] = key[r];
-        vout[i] = val[r];
+        kout[off + i] = key[r];
+        vout[off + i] = val[r];
       }
     }
-    return;
   }
-  const int rb = (bits + passes - 1) / passes, R = 1 << rb;
-  const bool direct = (size_t)G * R <= 32768; /* small table: each CTA scans it itself */
-  for (int pass = 0; pass < passes; ++pass) {
+  const int rb = (0 == passes) ? 0 : (bits + passes - 1) / passes, R = 1 << rb;
+  const bool direct = (size_t)rows_max * kRadix <= 32768; /* small tables: each CTA scans its stack's rows */
+  for (int pass = 0; pass < passes_all; ++pass) {
+    const bool active = pass < passes;
     const int shift = pass * rb;
     const bool last = (pass + 1 == passes);
     unsigned* const kdst = last ? kout : ((0 == (pass & 1)) ? k1 : k0);
@@ -248,7 +272,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int*
     int dig[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) {
-      dig[r] = (w0 + lane + 32 * r < w1) ? (int)((bucket_of(key[r], cmin, inv_g) >> shift) & (R - 1)) : kRadix;
+      dig[r] = (active && w0 + lane + 32 * r < w1) ? (int)((bucket_of(key[r], cmin, inv_g) >> shift) & (R - 1)) : kRadix;
     }
     /* (a) tile histogram, row hist[tile][0..R); per-warp counters zeroed for (c) */
     for (int d = threadIdx.x; d < R; d += blockDim.x) s_base[d] = 0;
@@ -261,75 +285,81 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int*
       if (kRadix != dig[r]) atomicAdd(&s_base[dig[r]], 1);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < R; d += blockDim.x) hist[(size_t)tile * R + d] = s_base[d];
+    for (int d = threadIdx.x; d < R; d += blockDim.x) hist[(size_t)tile * kRadix + d] = s_base[d];
     if (0 == pass) XS_STAMP(3);
     if (!grid_sync(ctl)) return;
     if (0 == pass) XS_STAMP(4);
-    /* (b) digit bases of this tile. Data written by other CTAs in this kernel is read with __ldcg
-       (from L2), never through a possibly stale L1 line; table reads are unrolled by 8. */
-    /* thread i owns digits [i*per, (i+1)*per): all threads share the R digits */
+    /* (b) digit bases of this tile inside its stack. Data written by other CTAs in this kernel is
+       read with __ldcg (from L2), never through a possibly stale L1 line. Thread i owns digits
+       [i*per, (i+1)*per). */
     constexpr int PER = kRadix / kSortThreads;
     const int per = (R + kSortThreads - 1) / kSortThreads;
     int tot[PER], pre[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) tot[j] = pre[j] = 0;
     if (direct) {
-      for (int tt = 0; tt < G; tt += 8) {
-        int h[8][PER];
+      if (active) {
+        for (int tt = 0; tt < G; tt += 8) {
+          int h[8][PER];
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+          for (int u = 0; u < 8; ++u)
 #pragma unroll
-          for (int j = 0; j < PER; ++j) {
-            const int d = threadIdx.x * per + j;
-            h[u][j] = (j < per && tt + u < G && d < R) ? __ldcg(hist + (size_t)(tt + u) * R + d) : 0;
-          }
+            for (int j = 0; j < PER; ++j) {
+              const int d = threadIdx.x * per + j;
+              h[u][j] = (j < per && tt + u < G && d < R) ? __ldcg(hist + (size_t)(tb + tt + u) * kRadix + d) : 0;
+            }
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+          for (int u = 0; u < 8; ++u)
 #pragma unroll
-          for (int j = 0; j < PER; ++j) {
-            tot[j] += h[u][j];
-            pre[j] += (tt + u < tile) ? h[u][j] : 0;
-          }
+            for (int j = 0; j < PER; ++j) {
+              tot[j] += h[u][j];
+              pre[j] += (tt + u < lt) ? h[u][j] : 0;
+            }
+        }
       }
     }
-    else { /* one owner warp per digit scans its column in place (32 tiles per step, all loads issued
-              first), totals to the extra row G */
-      for (int d = tile * kSortWarps + warp; d < R; d += G * kSortWarps) {
-        constexpr int kMaxSteps = 8; /* G <= 256 tiles */
-        int h[kMaxSteps];
+    else { /* owner warps: one per (stack, digit), scanning that stack's tile column in place (32
+              tiles per step, all loads issued first); totals to the stack's totals row */
+      for (int q = tile * kSortWarps + warp; q < desc.nstacks * kRadix; q += ntiles_all * kSortWarps) {
+        const int s2 = q / kRadix, d = q - s2 * kRadix;
+        if (d >= s_radix[s2]) continue; /* digits the stack does not use */
+        const int tb2 = desc.tile_begin[s2], G2 = desc.ntiles[s2];
+        constexpr int kSteps = kMaxGroupTiles / 32;
+        int h[kSteps];
 #pragma unroll
-        for (int q = 0; q < kMaxSteps; ++q) {
-          const int tt = 32 * q + lane;
-          h[q] = (tt < G) ? __ldcg(hist + (size_t)tt * R + d) : 0;
+        for (int st = 0; st < kSteps; ++st) {
+          const int tt = 32 * st + lane;
+          h[st] = (tt < G2) ? __ldcg(hist + (size_t)(tb2 + tt) * kRadix + d) : 0;
         }
         int run = 0;
 #pragma unroll
-        for (int q = 0; q < kMaxSteps; ++q) {
-          int x = h[q];
+        for (int st = 0; st < kSteps; ++st) {
+          int x = h[st];
 #pragma unroll
           for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
           }
-          const int tt = 32 * q + lane;
-          if (tt < G) hist[(size_t)tt * R + d] = run + x - h[q];
+          const int tt = 32 * st + lane;
+          if (tt < G2) hist[(size_t)(tb2 + tt) * kRadix + d] = run + x - h[st];
           run += __shfl_sync(0xffffffffu, x, 31);
         }
-        if (0 == lane) hist[(size_t)G * R + d] = run;
+        if (0 == lane) hist[(size_t)(ntiles_all + s2) * kRadix + d] = run;
       }
       if (!grid_sync(ctl)) return;
 #pragma unroll
       for (int j = 0; j < PER; ++j) {
         const int d = threadIdx.x * per + j;
-        tot[j] = (j < per && d < R) ? __ldcg(hist + (size_t)G * R + d) : 0;
-        pre[j] = (j < per && d < R) ? __ldcg(hist + (size_t)tile * R + d) : 0;
+        const bool ok = active && j < per && d < R;
+        tot[j] = ok ? __ldcg(hist + (size_t)(ntiles_all + si) * kRadix + d) : 0;
+        pre[j] = ok ? __ldcg(hist + (size_t)tile * kRadix + d) : 0;
       }
     }
     block_exscan<PER>(tot, s_wsum);
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
       const int d = threadIdx.x * per + j;
-      if (j < per && d < R) s_base[d] = tot[j] + pre[j];
+      if (j < per && d < R) s_base[d] = off + tot[j] + pre[j];
     }
     if (0 == pass) XS_STAMP(5);
     /* (c) stable scatter: per-warp counts -> per-warp offsets -> ordered placement */
@@ -366,14 +396,16 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(const int*
       __syncwarp();
     }
     if (0 == pass) XS_STAMP(6);
-    if (!last) {
+    if (pass + 1 < passes_all) {
       if (!grid_sync(ctl)) return;
+      if (pass + 1 < passes) {
 #pragma unroll
-      for (int r = 0; r < E; ++r) {
-        const int i = w0 + lane + 32 * r;
-        if (i < w1) {
-          key[r] = __ldcg(kdst + i);
-          val[r] = __ldcg(vdst + i);
+        for (int r = 0; r < E; ++r) {
+          const int i = w0 + lane + 32 * r;
+          if (i < w1) {
+            key[r] = __ldcg(kdst + off + i);
+            val[r] = __ldcg(vdst + off + i);
+          }
         }
       }
     }
@@ -393,57 +425,117 @@ int sort_grid_max(void) {
     if (cudaSuccess != cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, xs_stack_group_kernel<16>, kSortThreads, 0)) b = 1;
     const int per_sm = a < b ? a : b;
     grid = xs_sm_count() * (per_sm < 1 ? 1 : per_sm);
-    if (grid > 256) grid = 256; /* the owner-warp digit scan covers at most 256 tiles */
   }
   return grid;
 }
 
-/* Tiles: as few as possible of at most kTileSmall entries, or of kTileLarge when the stack needs more
-   tiles than fit on the device. Returns the grid (0 if the stack is larger than one launch takes). */
-int sort_grid(int S, int* large) {
+/* Tiles of a batch: kTileSmall entries each, or kTileLarge when the small tiles do not fit on the
+   device at once or one stack would need more than kMaxGroupTiles of them. Fills ntiles/tile_begin
+   and returns the grid (0 if the batch is larger than one launch takes). */
+int plan_tiles(xs_sort_batch_t* d, int* large) {
   const int gmax = sort_grid_max();
-  int grid = (S + kTileSmall - 1) / kTileSmall;
-  *large = 0;
-  if (grid > gmax) {
-    grid = (S + kTileLarge - 1) / kTileLarge;
-    *large = 1;
-    if (grid > gmax) return 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int T = pass ? kTileLarge : kTileSmall;
+    int total = 0, fits = 1;
+    for (int s = 0; s < d->nstacks; ++s) {
+      const int nt = (d->S[s] + T - 1) / T;
+      d->ntiles[s] = nt < 1 ? 1 : nt;
+      d->tile_begin[s] = total;
+      total += d->ntiles[s];
+      if (d->ntiles[s] > kMaxGroupTiles) fits = 0;
+    }
+    if (fits && total <= gmax) {
+      *large = pass;
+      return total;
+    }
   }
-  return grid < 1 ? 1 : grid;
+  return 0;
+}
+
+int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long* v0, unsigned* k1, unsigned long long* v1,
+  unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, cudaStream_t s, unsigned long long* stamps,
+  int clear_ctl) {
+  xs_sort_batch_t desc = desc0;
+  int large = 0;
+  const int grid = plan_tiles(&desc, &large);
+  if (0 == grid) return (int)cudaErrorInvalidValue; /* callers split batches above the launch limit */
+  SortCtl* ctl = (SortCtl*)sort_scratch;
+  int* hist = (int*)((char*)sort_scratch + xs_sort_ctl_bytes());
+  if (clear_ctl) {
+    int ng = 0;
+    for (int i = 0; i < desc.nstacks; ++i) ng = desc.gidx[i] + 1 > ng ? desc.gidx[i] + 1 : ng;
+    const cudaError_t r = cudaMemsetAsync(ctl, 0, sizeof(SortCtl) * (size_t)(1 + ng), s);
+    if (cudaSuccess != r) return (int)r;
+  }
+  void* args[] = {&desc, &k0, &v0, &k1, &v1, &kout, &vout, &seglist, &hist, &ctl, &stamps};
+  return (int)cudaLaunchCooperativeKernel(
+    large ? (const void*)xs_stack_group_kernel<16> : (const void*)xs_stack_group_kernel<8>, dim3(grid), dim3(kSortThreads),
+    args, 0, s);
 }
 
 }  // namespace
 
 extern "C" {
 
-size_t xs_stack_sort_scratch_bytes(int S) {
-  int large = 0;
-  const size_t G = (size_t)sort_grid(S, &large);
-  return sizeof(SortCtl) + 256 + sizeof(int) * ((G + 1) * kRadix);
+size_t xs_sort_ctl_bytes(void) { return (sizeof(SortCtl) * (1 + XS_MAX_CALL_STACKS) + 255) / 256 * 256; }
+
+int xs_sort_clear_ctl(void* sort_scratch, int nstacks, void* stream) {
+  return (int)cudaMemsetAsync(sort_scratch, 0, sizeof(SortCtl) * (size_t)(1 + nstacks), (cudaStream_t)stream);
 }
 
-int xs_stack_group_max(void) { return sort_grid_max() * kTileLarge; }
-
-static int xs_stack_group_impl(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
-  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream,
-  unsigned long long* stamps) {
-  cudaStream_t s = (cudaStream_t)stream;
-  SortCtl* ctl = (SortCtl*)sort_scratch;
-  int* hist = (int*)((char*)sort_scratch + sizeof(SortCtl) + 256);
+size_t xs_stack_sort_scratch_bytes_batch(const xs_sort_batch_t* desc) {
+  xs_sort_batch_t d = *desc;
   int large = 0;
-  int grid = sort_grid(S, &large);
-  if (0 == grid) return (int)cudaErrorInvalidValue; /* callers split stacks above xs_stack_group_max() */
-  cudaError_t r = cudaMemsetAsync(ctl, 0, sizeof(SortCtl), s);
-  if (cudaSuccess != r) return (int)r;
-  void* args[] = {&dev_stack, &S, &k0, &v0, &k1, &v1, &kout, &vout, &seglist, &hist, &ctl, &stamps};
-  return (int)cudaLaunchCooperativeKernel(
-    large ? (const void*)xs_stack_group_kernel<16> : (const void*)xs_stack_group_kernel<8>, dim3(grid), dim3(kSortThreads),
-    args, 0, s);
+  const int grid = plan_tiles(&d, &large);
+  const size_t rows = (size_t)(grid > 0 ? grid : sort_grid_max()) + (size_t)XS_MAX_BATCH;
+  return xs_sort_ctl_bytes() + sizeof(int) * rows * kRadix;
+}
+
+int xs_stack_group_fits(const xs_sort_batch_t* desc) {
+  xs_sort_batch_t d = *desc;
+  int large = 0;
+  return plan_tiles(&d, &large) > 0 ? 1 : 0;
+}
+
+size_t xs_stack_sort_scratch_bytes(int S) {
+  xs_sort_batch_t d;
+  d.nstacks = 1;
+  d.S[0] = S;
+  return xs_stack_sort_scratch_bytes_batch(&d);
+}
+
+int xs_stack_group_max(void) { return (sort_grid_max() < kMaxGroupTiles ? sort_grid_max() : kMaxGroupTiles) * kTileLarge; }
+
+int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
+  return group_launch(*desc, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, (cudaStream_t)stream, nullptr, 0);
 }
 
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
-  return xs_stack_group_impl(dev_stack, S, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, stream, nullptr);
+  xs_sort_batch_t d;
+  d.nstacks = 1;
+  d.stack[0] = dev_stack;
+  d.S[0] = S;
+  d.off[0] = 0;
+  d.gidx[0] = 0;
+  return group_launch(d, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, (cudaStream_t)stream, nullptr, 1);
+}
+
+unsigned* xs_sort_queue_counter(void* sort_scratch) { return &((SortCtl*)sort_scratch)->queue; }
+const unsigned* xs_sort_error_flag(void* sort_scratch) { return &((SortCtl*)sort_scratch)->err; }
+int xs_sort_launch_tiles(void) { return sort_grid_max() < kMaxGroupTiles ? sort_grid_max() : kMaxGroupTiles; }
+int xs_sort_tile_entries(int large) { return large ? kTileLarge : kTileSmall; }
+
+int libxstream_b200_device_error(int reset) {
+  unsigned e = 0;
+  if (EXIT_SUCCESS != xs_ensure_device()) return -1;
+  if (cudaSuccess != cudaMemcpyFromSymbol(&e, xs_device_error_word, sizeof(e))) return -1;
+  if (0 != reset && 0 != e) {
+    const unsigned zero = 0;
+    if (cudaSuccess != cudaMemcpyToSymbol(xs_device_error_word, &zero, sizeof(zero))) return -1;
+  }
+  return (int)e;
 }
 
 /* Diagnostic variant: the grouping of one stack with per-CTA phase timestamps (ns, %globaltimer)
@@ -451,13 +543,20 @@ int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long
    number of tiles (CTAs), or a negative CUDA error code. */
 int xs_stack_group_profile(const int* dev_stack, int S, unsigned long long* host_stamps, int capacity, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
+  xs_sort_batch_t d;
+  d.nstacks = 1;
+  d.stack[0] = dev_stack;
+  d.S[0] = S;
+  d.off[0] = 0;
+  d.gidx[0] = 0;
+  xs_sort_batch_t dp = d;
   int large = 0;
-  const int grid = sort_grid(S, &large);
+  const int grid = plan_tiles(&dp, &large);
   if (0 == grid || capacity < grid * 8) return -(int)cudaErrorInvalidValue;
   const size_t ks = sizeof(unsigned) * (size_t)S, vs = sizeof(unsigned long long) * (size_t)S;
   char* buf = nullptr;
   const size_t scr = xs_stack_sort_scratch_bytes(S);
-  const size_t total = 3 * ks + 3 * vs + sizeof(int) * 2 + scr + 8 * sizeof(unsigned long long) * grid + 4096;
+  const size_t total = 3 * ks + 3 * vs + scr + 8 * sizeof(unsigned long long) * grid + 8192;
   cudaError_t r = cudaMallocAsync((void**)&buf, total, s);
   if (cudaSuccess != r) return -(int)r;
   char* p = buf;
@@ -471,20 +570,11 @@ int xs_stack_group_profile(const int* dev_stack, int S, unsigned long long* host
   unsigned long long* st = (unsigned long long*)p; p += 8 * sizeof(unsigned long long) * grid;
   int* seg = (int*)p; p += 256;
   p = (char*)(((uintptr_t)p + 255) & ~(uintptr_t)255);
-  int rc = xs_stack_group_impl(dev_stack, S, k0, v0, k1, v1, ko, vo, seg, p, s, st);
+  int rc = group_launch(d, k0, v0, k1, v1, ko, vo, seg, p, s, st, 1);
   if (0 == rc) rc = (int)cudaMemcpyAsync(host_stamps, st, 8 * sizeof(unsigned long long) * grid, cudaMemcpyDeviceToHost, s);
   cudaFreeAsync(buf, s);
   if (cudaSuccess == (cudaError_t)rc) rc = (int)cudaStreamSynchronize(s);
   return (0 == rc) ? grid : -rc;
-}
-
-int xs_stack_sort_error(void* sort_scratch, int* err, void* stream) {
-  SortCtl* ctl = (SortCtl*)sort_scratch;
-  unsigned e = 0;
-  cudaError_t r = cudaMemcpyAsync(&e, &ctl->err, sizeof(e), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
-  if (cudaSuccess == r) r = cudaStreamSynchronize((cudaStream_t)stream);
-  *err = (int)e;
-  return (int)r;
 }
 
 }  // extern "C"
