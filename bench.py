@@ -49,6 +49,9 @@ def parse_args():
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end arm (default: min(steps, 50))")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["stack23", "mixed", "mixed2m"], default="stack23",
+                   help="stack23: the 23x23x23 stack (default); mixed / mixed2m: 12 mixed-shape stacks in one "
+                        "batch call replayed as a CUDA graph (stated sizes / scaled to 2M triples)")
     return p.parse_args()
 
 
@@ -346,12 +349,144 @@ def run_b200(args, d: Dist):
         print(json.dumps(line), flush=True)
 
 
+def run_mixed(args, d: Dist):
+    """Mixed-shape batch: one libxstream_b200_process_batch call per step, captured once into a CUDA
+    graph and replayed; compared with one libsmm_acc_process per stack; plus the transpose set."""
+    import ctypes
+
+    import libxstream_b200 as xs
+    from libxstream_b200 import StackDesc
+    from libxstream_b200 import acc as A
+    from libxstream_b200 import workloads as W
+
+    L = xs.lib()
+    if d.world > 1:
+        xs.check(L.c_dbcsr_acc_set_active_device(d.local_rank), "set_active_device")
+    A.init()
+    cases = W.mixed_shapes() if args.workload == "mixed" else W.mixed_shapes_scaled()
+    stream = A.Stream("bench")
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
+    bufs, descs = [], []
+    for c in cases:
+        da, db = A.DevBuf.from_array(c.a, stream), A.DevBuf.from_array(c.b_rowmajor(), stream)
+        ds, dc = A.DevBuf.from_array(c.stack, stream), A.DevBuf(c.nc * c.m * c.n * 8)
+        dc.zero(stream)
+        bufs.append((da, db, ds, dc))
+        descs.append(StackDesc(ds.ptr, c.S, c.m, c.n, c.k, da.ptr, db.ptr, dc.ptr))
+    arr = (StackDesc * len(descs))(*descs)
+    flops = sum(c.flops for c in cases)
+    flush = A.DevBuf(FLUSH_BYTES)
+    ev = []
+    for _ in range(2 * args.steps):
+        e = ctypes.c_void_p()
+        xs.check(L.libxstream_b200_event_create_timed(ctypes.byref(e)), "event")
+        ev.append(e.value)
+
+    def timed(step_fn):
+        for _ in range(max(args.warmup, 3)):
+            flush.zero(stream)
+            step_fn()
+        stream.sync()
+        d.barrier()
+        for i in range(args.steps):
+            flush.zero(stream)
+            L.c_dbcsr_acc_event_record(ev[2 * i], stream.handle)
+            step_fn()
+            L.c_dbcsr_acc_event_record(ev[2 * i + 1], stream.handle)
+        stream.sync()
+        d.barrier()
+        return d.max(sum(L.libxstream_b200_event_elapsed_ms(ev[2 * i], ev[2 * i + 1]) for i in range(args.steps))) / args.steps
+
+    gexec, nk = ctypes.c_void_p(), ctypes.c_int(0)
+    xs.check(L.libxstream_b200_process_batch(ctypes.cast(arr, ctypes.c_void_p), len(descs), 80, stream.handle), "batch")
+    stream.sync()
+    xs.check(L.libxstream_b200_graph_begin(stream.handle), "graph_begin")
+    rc = L.libxstream_b200_process_batch(ctypes.cast(arr, ctypes.c_void_p), len(descs), 80, stream.handle)
+    xs.check(L.libxstream_b200_graph_end(stream.handle, ctypes.byref(gexec), ctypes.byref(nk)), "graph_end")
+    xs.check(rc, "batch (capture)")
+    ms_graph = timed(lambda: xs.check(L.libxstream_b200_graph_launch(gexec, stream.handle), "graph_launch"))
+    ms_batch = timed(lambda: xs.check(L.libxstream_b200_process_batch(ctypes.cast(arr, ctypes.c_void_p), len(descs), 80,
+                                                                      stream.handle), "batch"))
+
+    def per_stack():
+        for c, (da, db, ds, dc) in zip(cases, bufs):
+            xs.check(A.process(ds, c.S, da, db, dc, c.m, c.n, c.k, stream), "process")
+    ms_single = timed(per_stack)
+
+    def breakdown(step_fn):
+        """Per-kernel device time of one step (launch profile events; a separate, untimed pass)."""
+        L.libxstream_b200_profile_reset()
+        L.libxstream_b200_profile_enable(1)
+        for _ in range(5):
+            flush.zero(stream)
+            step_fn()
+        stream.sync()
+        L.libxstream_b200_profile_enable(0)
+        out = {}
+        for name in ("sort", "smm_batch", "combine_batch", "smm", "combine"):
+            nl, ms, gf, gb = ctypes.c_long(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            if L.libxstream_b200_profile_query(name.encode(), ctypes.byref(nl), ctypes.byref(ms), ctypes.byref(gf),
+                                               ctypes.byref(gb)) == 0 and nl.value > 0:
+                out[name] = {"launches_per_step": nl.value / 5, "ms_per_step": ms.value / 5}
+        return out
+    prof_batch = breakdown(lambda: xs.check(L.libxstream_b200_process_batch(ctypes.cast(arr, ctypes.c_void_p),
+                                                                            len(descs), 80, stream.handle), "batch"))
+    prof_single = breakdown(per_stack)
+    L.libxstream_b200_graph_destroy(gexec)
+    # transposes: 100k square blocks of 5..64, one libsmm_acc_transpose call per size
+    tw = W.transpose_workload()
+    tbufs = []
+    for size, count in tw.items():
+        data = A.DevBuf(count * size * size * 8)
+        data.zero(stream)
+        trs = A.DevBuf.from_array(np.arange(count, dtype=np.int32) * (size * size), stream)
+        tbufs.append((size, count, data, trs))
+
+    def transposes():
+        for size, count, data, trs in tbufs:
+            xs.check(A.transpose(trs, 0, count, data, size, size, stream), "transpose")
+    ms_trans = timed(transposes)
+    tbytes = sum(16 * s * s * c for s, c in tw.items())
+    clocks = sampler.stop()
+    value = d.world * flops / (ms_graph * 1e-3) * 1e-9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mixed-shape batch: {len(cases)} FP64 stacks, (m,n,k) from "
+                                   f"{list(W.MIXED_SHAPE_SET)}^3, {sum(c.S for c in cases)} triples "
+                                   + ("(sizes log-uniform 100..200000)" if args.workload == "mixed"
+                                      else "(log-uniform sizes scaled to 2M triples)"),
+                       "shapes": [[c.m, c.n, c.k, c.S] for c in cases], "gflop_per_step": flops * 1e-9,
+                       "l2": "flushed between timed steps (256 MiB memset, outside the timed events)"},
+            "batch_graph": {"ms": ms_graph, "gflops": flops / (ms_graph * 1e-3) * 1e-9, "kernels": nk.value},
+            "batch_direct": {"ms": ms_batch, "gflops": flops / (ms_batch * 1e-3) * 1e-9,
+                             "kernel_profile": prof_batch},
+            "per_stack_calls": {"ms": ms_single, "gflops": flops / (ms_single * 1e-3) * 1e-9,
+                                "calls": len(cases), "kernel_profile": prof_single},
+            "transpose": {"blocks": sum(tw.values()), "calls": len(tw), "ms": ms_trans,
+                          "gbs": tbytes / (ms_trans * 1e-3) * 1e-9, "bytes": tbytes},
+            "gpu_launches": nk.value * args.steps, "clocks": clocks}
+    for bset in bufs:
+        for b in bset:
+            b.free()
+    for _, _, data, trs in tbufs:
+        data.free()
+        trs.free()
+    flush.free()
+    stream.destroy()
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     d = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, d)
+        elif args.workload != "stack23":
+            run_mixed(args, d)
         else:
             run_b200(args, d)
     finally:

@@ -105,9 +105,10 @@ int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
 int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
-/** Device addresses inside the sort scratch: the work-queue counter (zeroed with the statistics
-    at every call) and the error flag a timed-out grid barrier sets. */
-unsigned* xs_sort_queue_counter(void* sort_scratch);
+/** Device addresses inside the sort scratch: the work-queue counters of the stack kernels (one per
+    tile-class group 0..3, zeroed with the statistics at every call) and the error flag a timed-out
+    grid barrier sets. */
+unsigned* xs_sort_queue_counter(void* sort_scratch, int which);
 const unsigned* xs_sort_error_flag(void* sort_scratch);
 
 /** Batch of stacks (include/libxstream_b200.h: libxstream_b200_stack_t): scratch size and launch. */

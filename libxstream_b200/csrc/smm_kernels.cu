@@ -332,27 +332,35 @@ struct BatchTasks {
   StackTask t[kMaxBatchTasks];
 };
 
+/* Register groups of the batch: group 0 holds the tile classes with MT*NT <= 9 fragments (168
+   registers, 3 CTAs per SM), group 1 the larger ones (255 registers, 2 CTAs per SM). */
+__host__ __device__ constexpr int batch_group(int mt, int nt) { return (mt * nt <= 9) ? 0 : 1; }
+__host__ __device__ constexpr int batch_group_min_blocks(int grp) { return (0 == grp) ? 3 : 2; }
+__host__ __device__ constexpr int batch_group_max_frags(int grp) { return (0 == grp) ? 9 : 16; }
+/* k-steps per register panel: 4 for small tiles, 2 for mid-size, 1 for the largest (whose
+   accumulators alone take 48-64 registers) */
+__host__ __device__ constexpr int batch_kp(int mt, int nt) { return (mt * nt <= 4) ? 4 : ((mt * nt < 12) ? 2 : 1); }
+
 /* One tile class of the batch kernel as a separate (not inlined) function, so that each class gets
-   its own register allocation instead of sharing one with the other classes' code. The largest
-   tiles keep one k-step per register panel: their accumulators alone take 48-64 registers. */
+   its own register allocation instead of sharing one with the other classes' code. */
 template <int MT, int NT>
 __device__ __noinline__ void batch_item(const StackTask& tk, int group, int sub, int* seglist, double* smem) {
-  smm_item<0, 0, 0, MT, NT, (MT * NT >= 12) ? 1 : 2>(tk, group, sub, seglist, smem);
+  smm_item<0, 0, 0, MT, NT, batch_kp(MT, NT)>(tk, group, sub, seglist, smem);
 }
 
-template <int X, int MT, int NT>
+template <int GRP, int MT, int NT>
 __device__ __forceinline__ void batch_dispatch(int cls, const StackTask& tk, int group, int sub, int* seglist, double* smem) {
-  if constexpr (MT <= X && NT <= X) {
+  if constexpr (batch_group(MT, NT) == GRP) {
     if ((MT - 1) * 4 + (NT - 1) == cls) batch_item<MT, NT>(tk, group, sub, seglist, smem);
   }
 }
 
-/* Persistent batch kernel: one launch for all stacks of a multiplication. The grid is the number of
-   CTAs resident on the device; each CTA takes work items (CTA group x sub-tile of one stack) from a
-   global queue, in the order the host sorted them (heaviest items first), and runs them with the
-   tile class of their stack (any MT, NT <= X). */
-template <int X>
-__global__ void __launch_bounds__(128, smm_min_blocks(X, X))
+/* Persistent batch kernel of one register group: one launch for all stacks of the group. The grid is
+   the number of CTAs resident on the device; each CTA takes work items (CTA group x sub-tile of one
+   stack) from the group's queue, in the order the host sorted them (heaviest items first), and runs
+   them with the tile class of their stack. */
+template <int GRP>
+__global__ void __launch_bounds__(128, batch_group_min_blocks(GRP))
   xs_smm_batch_kernel(const __grid_constant__ BatchTasks bt, int* __restrict__ seglist, unsigned* __restrict__ queue,
     const unsigned* __restrict__ err) {
   extern __shared__ double smem[];
@@ -369,22 +377,22 @@ __global__ void __launch_bounds__(128, smm_min_blocks(X, X))
     const StackTask& tk = bt.t[ti];
     const int local = item - tk.item_begin, group = local / tk.nsub, sub = local - group * tk.nsub;
     const int cls = tk.cls;
-    batch_dispatch<X, 1, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 1, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 1, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 1, 4>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 2, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 2, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 2, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 2, 4>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 3, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 3, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 3, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 3, 4>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 4, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 4, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 4, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<X, 4, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 1, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 1, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 1, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 1, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 2, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 2, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 2, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 2, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 3, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 3, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 3, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 3, 4>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 4, 1>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 4, 2>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 4, 3>(cls, tk, group, sub, seglist, smem);
+    batch_dispatch<GRP, 4, 4>(cls, tk, group, sub, seglist, smem);
   }
 }
 
@@ -520,6 +528,7 @@ __global__ void __launch_bounds__(32 * kCombineWarps)
 
 struct SmmPlan {
   int nsub_m, nsub_n, nsub, nchunks, L, W, ngroups;
+  int no_combine; /* the stack kernel only: CTA-crossing pieces are combined by the caller */
   size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces;
   size_t off_sort, total;
 };
@@ -538,6 +547,7 @@ launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm);
 int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl) {
   const int mt = prm->mt, nt = prm->nt;
   if (mt < 1 || mt > 4 || nt < 1 || nt > 4) return -1;
+  pl->no_combine = 0;
   pl->nsub_m = ((m + 7) / 8 + mt - 1) / mt;
   pl->nsub_n = ((n + 7) / 8 + nt - 1) / nt;
   pl->nsub = pl->nsub_m * pl->nsub_n;
@@ -599,6 +609,7 @@ cudaError_t launch_dmma(const SmmPlan& pl, const StackTask& tk, int* seglist, co
   if (cudaSuccess != r) return r;
   const double m = tk.m, n = tk.n, k = tk.k;
   xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
+  if (pl.no_combine) return cudaSuccess;
   const int cgrid = max(1, min(pl.ngroups * pl.nsub, 2 * xs_sm_count()));
   const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (MT * NT * 2) * 32;
   if (!csmem_set) {
@@ -648,20 +659,18 @@ launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
 
 constexpr int kBatchW = 4; /* warps per CTA of the batch kernel */
 
-size_t batch_smem_bytes(int X) { return (size_t)kBatchW * (2 * X * X * 2 * 32 * sizeof(double) + 4 * sizeof(int)); }
+size_t batch_smem_bytes(int grp) {
+  return (size_t)kBatchW * (2 * batch_group_max_frags(grp) * 2 * 32 * sizeof(double) + 4 * sizeof(int));
+}
 
-template <int X>
+template <int GRP>
 cudaError_t batch_prepare(int* occ) {
   static int done = 0, occ_cached = 0;
   cudaError_t r = cudaSuccess;
   if (!done) {
-    const size_t smem = batch_smem_bytes(X);
-    const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32;
-    if (smem > 48 * 1024) r = cudaFuncSetAttribute(xs_smm_batch_kernel<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaSuccess == r && csmem > 48 * 1024) {
-      r = cudaFuncSetAttribute(xs_smm_combine_batch_kernel<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
-    }
-    if (cudaSuccess == r) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_cached, xs_smm_batch_kernel<X>, 32 * kBatchW, smem);
+    const size_t smem = batch_smem_bytes(GRP);
+    if (smem > 48 * 1024) r = cudaFuncSetAttribute(xs_smm_batch_kernel<GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaSuccess == r) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_cached, xs_smm_batch_kernel<GRP>, 32 * kBatchW, smem);
     if (cudaSuccess != r) return r;
     done = 1;
   }
@@ -669,28 +678,44 @@ cudaError_t batch_prepare(int* occ) {
   return r;
 }
 
-cudaError_t batch_occupancy(int X, int* occ) {
-  switch (X) {
-    case 1: return batch_prepare<1>(occ);
-    case 2: return batch_prepare<2>(occ);
-    case 3: return batch_prepare<3>(occ);
-    default: return batch_prepare<4>(occ);
-  }
-}
+cudaError_t batch_occupancy(int grp, int* occ) { return (0 == grp) ? batch_prepare<0>(occ) : batch_prepare<1>(occ); }
 
 template <int X>
-cudaError_t batch_run(const BatchTasks& bt, int ngroups_total, int* seglist, unsigned* queue, const unsigned* err,
-  double flops, double bytes, cudaStream_t s) {
+cudaError_t combine_prepare(void) {
+  static int done = 0;
+  if (!done) {
+    const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32;
+    if (csmem > 48 * 1024) {
+      const cudaError_t r = cudaFuncSetAttribute(xs_smm_combine_batch_kernel<X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)csmem);
+      if (cudaSuccess != r) return r;
+    }
+    done = 1;
+  }
+  return cudaSuccess;
+}
+
+/* Persistent stack kernel of register group GRP over the tasks in bt (their own work queue). */
+template <int GRP>
+cudaError_t batch_smm(const BatchTasks& bt, int* seglist, unsigned* queue, const unsigned* err, double flops, double bytes,
+  cudaStream_t s) {
   int occ = 0;
-  cudaError_t r = batch_prepare<X>(&occ);
+  cudaError_t r = batch_prepare<GRP>(&occ);
   if (cudaSuccess != r) return r;
   const int grid = max(1, min(bt.nitems, max(1, occ) * xs_sm_count()));
   void* prof = xs_profile_begin(s);
-  xs_smm_batch_kernel<X><<<grid, 32 * kBatchW, batch_smem_bytes(X), s>>>(bt, seglist, queue, err);
+  xs_smm_batch_kernel<GRP><<<grid, 32 * kBatchW, batch_smem_bytes(GRP), s>>>(bt, seglist, queue, err);
   r = cudaGetLastError();
-  if (cudaSuccess != r) return r;
   xs_profile_end(prof, "smm_batch", flops, bytes, s);
-  prof = xs_profile_begin(s);
+  return r;
+}
+
+/* Combine of all CTA-crossing segments of the batch (bt: every task of the call). */
+template <int X>
+cudaError_t batch_combine(const BatchTasks& bt, int ngroups_total, int* seglist, const unsigned* err, cudaStream_t s) {
+  cudaError_t r = combine_prepare<X>();
+  if (cudaSuccess != r) return r;
+  void* prof = xs_profile_begin(s);
   const int cgrid = max(1, min(ngroups_total, 2 * xs_sm_count()));
   xs_smm_combine_batch_kernel<X><<<cgrid, 32 * kCombineWarps, sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32, s>>>(
     bt, kBatchW, seglist, err);
@@ -705,8 +730,14 @@ struct BatchPart {
   int first; /* first entry of the slice */
   int S;
   int mt, nt;
+  int solo; /* large enough to fill the device alone: runs as its own (shape-specialised) launch */
   double item_cost;
+  xs_smm_params_t prm;
 };
+
+/* A part whose one-wave chunk length (as a launch of its own) reaches this many entries keeps the
+   device busy by itself; it runs with the single-stack kernel of its shape instead of the queue. */
+constexpr int kSoloMinL = 16;
 
 struct BatchPlan {
   int nparts, X, ntotal, ngroups_total, nitems;
@@ -751,23 +782,39 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
       p.S = min(smax, st[i].stack_size - first);
       p.mt = prm.mt;
       p.nt = prm.nt;
+      p.prm = prm;
+      p.solo = 0;
       if (p.mt > bp->X) bp->X = p.mt;
       if (p.nt > bp->X) bp->X = p.nt;
       bp->ntotal += p.S;
     }
   }
   if (0 == bp->nparts) return 0;
-  int occ = 0;
-  if (cudaSuccess != batch_occupancy(bp->X, &occ) || occ < 1) occ = 1;
-  /* cost units: DMMA instructions per entry per warp plus a fixed per-entry overhead */
-  double total = 0;
+  /* large parts run alone, one wave of the single-stack kernel each; the rest share the queue.
+     Cost units: DMMA instructions per entry per warp plus a fixed per-entry overhead; each register
+     group gets items of equal cost, about two per CTA resident in that group's launch */
+  double total[2] = {0, 0};
+  int solo_L[kMaxBatchTasks];
   for (int q = 0; q < bp->nparts; ++q) {
-    const BatchPart& p = bp->part[q];
+    BatchPart& p = bp->part[q];
     const libxstream_b200_stack_t& d = st[p.stack];
     const int nsub = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
-    total += (double)p.S * nsub * (p.mt * p.nt * ((d.k + 3) / 4) + 8);
+    SmmPlan pl = {};
+    pl.W = kBatchW;
+    StackTask none = {};
+    int occ = 0;
+    if (cudaSuccess != find_launcher(d.m, d.n, d.k, &p.prm)(pl, none, nullptr, nullptr, 0, &occ) || occ < 1) occ = 1;
+    const long resident = (long)occ * xs_sm_count();
+    solo_L[q] = (int)(((long)p.S * nsub + resident * kBatchW - 1) / (resident * kBatchW));
+    p.solo = (solo_L[q] >= kSoloMinL) ? 1 : 0;
+    if (!p.solo) total[batch_group(p.mt, p.nt)] += (double)p.S * nsub * (p.mt * p.nt * ((d.k + 3) / 4) + 8);
   }
-  const double target = total / ((double)occ * xs_sm_count() * 4.0); /* cost of one work item */
+  double target[2];
+  for (int grp = 0; grp < 2; ++grp) {
+    int occ = 0;
+    if (cudaSuccess != batch_occupancy(grp, &occ) || occ < 1) occ = 1;
+    target[grp] = total[grp] / ((double)occ * xs_sm_count() * 2.0);
+  }
   size_t off = 0, poff = 0;
   bp->ngroups_total = 0;
   bp->nitems = 0;
@@ -777,7 +824,7 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     bp->nsub_n[q] = (((d.n + 7) / 8) + p.nt - 1) / p.nt;
     bp->nsub[q] = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * bp->nsub_n[q];
     const double per_entry = p.mt * p.nt * ((d.k + 3) / 4) + 8;
-    long L = (long)(target / (kBatchW * per_entry) + 0.5);
+    long L = p.solo ? solo_L[q] : (long)(target[batch_group(p.mt, p.nt)] / (kBatchW * per_entry) + 0.5);
     if (L < 1) L = 1;
     if (L > p.S) L = p.S;
     bp->L[q] = (int)L;
@@ -789,7 +836,7 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     bp->pieces_off[q] = poff;
     poff += (size_t)2 * bp->ngroups[q] * bp->nsub[q] * (p.mt * p.nt * 2) * 32;
     bp->ngroups_total += bp->ngroups[q];
-    bp->nitems += bp->ngroups[q] * bp->nsub[q];
+    if (!p.solo) bp->nitems += bp->ngroups[q] * bp->nsub[q];
     bp->order[q] = q;
   }
   for (int a = 1; a < bp->nparts; ++a) { /* heaviest items first (insertion sort, stable) */
@@ -1006,17 +1053,18 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     tiles += nt;
   }
   xs_profile_end(prof, "sort", 0.0, 48.0 * bp.ntotal, s);
-  BatchTasks bt;
-  memset(&bt, 0, sizeof(bt));
-  bt.ntasks = bp.nparts;
-  bt.nitems = bp.nitems;
-  double flops = 0, bytes = 0;
-  int item = 0;
+  /* task table of the whole call (for the combine); one launch of the single-stack kernel per solo
+     part and one persistent launch per register group for the others: every group runs at the
+     occupancy its largest tiles allow */
+  BatchTasks all, grp[2];
+  memset(&all, 0, sizeof(all));
+  memset(grp, 0, sizeof(grp));
+  double gflops[2] = {0, 0}, gbytes[2] = {0, 0};
   for (int i = 0; i < bp.nparts; ++i) {
     const int q = bp.order[i];
     const BatchPart& p = bp.part[q];
     const libxstream_b200_stack_t& d = st[p.stack];
-    StackTask& tk = bt.t[i];
+    StackTask tk = {};
     tk.a = (const double*)d.a;
     tk.b = (const double*)d.b;
     tk.c = (double*)d.c;
@@ -1032,20 +1080,45 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     tk.ngroups = bp.ngroups[q];
     tk.nsub_n = bp.nsub_n[q];
     tk.nsub = bp.nsub[q];
-    tk.item_begin = item;
     tk.cls = (p.mt - 1) * 4 + (p.nt - 1);
     tk.sid = q;
-    item += tk.ngroups * tk.nsub;
-    flops += 2.0 * d.m * d.n * d.k * (double)p.S;
-    bytes += 8.0 * p.S * ((double)d.m * d.k + (double)d.k * d.n + 2.0 * d.m * d.n);
+    tk.item_begin = all.nitems;
+    all.t[all.ntasks++] = tk;
+    all.nitems += tk.ngroups * tk.nsub;
+    if (p.solo) {
+      SmmPlan pl = {};
+      pl.W = kBatchW;
+      pl.L = tk.L;
+      pl.nchunks = tk.nchunks;
+      pl.ngroups = tk.ngroups;
+      pl.nsub_n = tk.nsub_n;
+      pl.nsub = tk.nsub;
+      pl.no_combine = 1;
+      r = (int)find_launcher(d.m, d.n, d.k, &p.prm)(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
+      if (0 != r) return r;
+      continue;
+    }
+    const int X = batch_group(p.mt, p.nt);
+    BatchTasks& b = grp[X];
+    tk.item_begin = b.nitems;
+    b.t[b.ntasks++] = tk;
+    b.nitems += tk.ngroups * tk.nsub;
+    gflops[X] += 2.0 * d.m * d.n * d.k * (double)p.S;
+    gbytes[X] += 8.0 * p.S * ((double)d.m * d.k + (double)d.k * d.n + 2.0 * d.m * d.n);
   }
-  unsigned* const queue = xs_sort_queue_counter(sort_scratch);
   const unsigned* const err = xs_sort_error_flag(sort_scratch);
+  for (int X = 0; X < 2 && 0 == r; ++X) {
+    if (0 == grp[X].ntasks) continue;
+    unsigned* const queue = xs_sort_queue_counter(sort_scratch, X);
+    r = (0 == X) ? (int)batch_smm<0>(grp[X], seglist, queue, err, gflops[X], gbytes[X], s)
+                 : (int)batch_smm<1>(grp[X], seglist, queue, err, gflops[X], gbytes[X], s);
+  }
+  if (0 != r) return r;
   switch (bp.X) {
-    case 1: return (int)batch_run<1>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
-    case 2: return (int)batch_run<2>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
-    case 3: return (int)batch_run<3>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
-    default: return (int)batch_run<4>(bt, bp.ngroups_total, seglist, queue, err, flops, bytes, s);
+    case 1: return (int)batch_combine<1>(all, bp.ngroups_total, seglist, err, s);
+    case 2: return (int)batch_combine<2>(all, bp.ngroups_total, seglist, err, s);
+    case 3: return (int)batch_combine<3>(all, bp.ngroups_total, seglist, err, s);
+    default: return (int)batch_combine<4>(all, bp.ngroups_total, seglist, err, s);
   }
 }
 

@@ -32,7 +32,8 @@ constexpr unsigned kSpinLimit = 1u << 24;
 constexpr int kMaxGroupTiles = 256; /* the owner-warp digit scan covers at most 256 tiles per stack */
 
 /* Control block of one call, zero-initialised by one memset at the start of the call:
-   ctl[0] holds the grid barrier, the error flag and the stack kernel's work-queue counter;
+   ctl[0] holds the grid barrier, the error flag and the stack kernels' work-queue counters (its four
+   statistics words serve as the queues of the tile-class groups 1..4, `queue` is spare);
    ctl[1 + g] the statistics of stack g of the call (the minimum kept as its complement, atomicMax). */
 struct SortCtl {
   unsigned ncmin, cmax, gcd, pad0;
@@ -522,7 +523,11 @@ int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long
   return group_launch(d, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, (cudaStream_t)stream, nullptr, 1);
 }
 
-unsigned* xs_sort_queue_counter(void* sort_scratch) { return &((SortCtl*)sort_scratch)->queue; }
+unsigned* xs_sort_queue_counter(void* sort_scratch, int which) {
+  SortCtl* const c = (SortCtl*)sort_scratch;
+  unsigned* const q[4] = {&c->ncmin, &c->cmax, &c->gcd, &c->pad0};
+  return q[which & 3];
+}
 const unsigned* xs_sort_error_flag(void* sort_scratch) { return &((SortCtl*)sort_scratch)->err; }
 int xs_sort_launch_tiles(void) { return sort_grid_max() < kMaxGroupTiles ? sort_grid_max() : kMaxGroupTiles; }
 int xs_sort_tile_entries(int large) { return large ? kTileLarge : kTileSmall; }

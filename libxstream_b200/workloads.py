@@ -146,6 +146,19 @@ def mixed_shapes(seed: int = SEED, nstacks: int = 12, smin: int = 100, smax: int
     return cases
 
 
+def mixed_shapes_scaled(total: int = 2_000_000, seed: int = SEED) -> list[StackCase]:
+    """The 12 mixed_shapes() stacks with every stack size multiplied by one common factor so that
+    the batch holds about `total` triples (the relative log-uniform spread is kept)."""
+    base = mixed_shapes(seed=seed)
+    scale = total / sum(c.S for c in base)
+    out = []
+    for i, c in enumerate(base):
+        S = max(1, int(round(c.S * scale)))
+        na, nb, nc = pool_sizes(S)
+        out.append(stack_case(c.m, c.n, c.k, S, na, nb, nc, seed=seed + 1 + i))
+    return out
+
+
 def transpose_workload(seed: int = SEED, nblocks: int = 100000, smin: int = 5, smax: int = 64):
     """Square blocks with sizes uniform in [smin, smax]: returns {size: count}."""
     g = rng(seed)
