@@ -117,6 +117,18 @@ int libxstream_b200_process_noalloc(const int* host_param_stack, const int* dev_
 size_t libxstream_b200_noalloc_scratch_bytes(void);
 size_t libxstream_b200_process_scratch_bytes(int stack_size, int m, int n, int k);
 
+/**
+ * Ozaki scheme-1 FP64 GEMM on the int8 tensor cores: C = alpha*op(A)*op(B) + beta*C with
+ * column-major device operands (op = 'N' or 'T'), each row of op(A) / column of op(B) split into
+ * nslices (1..8; <= 0 means 8) int8 digit slices under power-of-two scaling, slice pairs with
+ * sa + sb <= 2*(nslices-1) - trim multiplied with exact int32 sums and recombined in FP64.
+ * Replaces ozaki_gemm (samples/ozaki/ozaki_opencl.h:420-421; nslices and trim play the roles of
+ * ozaki_init's ndecomp and oztrim, ozaki_opencl.h:328-329) for Scheme 1. Enqueued on stream
+ * (NULL: the per-thread default stream); returns 0 on success.
+ */
+int libxstream_b200_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
+  const double* b, int ldb, double beta, double* c, int ldc, int nslices, int trim, void* stream);
+
 #if defined(__cplusplus)
 }
 #endif

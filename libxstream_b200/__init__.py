@@ -83,6 +83,10 @@ SIGNATURES = {
     "libxstream_b200_graph_end": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_int_p]),
     "libxstream_b200_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "libxstream_b200_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "libxstream_b200_ozaki_gemm": (ctypes.c_int, [ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "libxstream_b200_process_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

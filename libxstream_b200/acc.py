@@ -156,3 +156,11 @@ def get_params(m: int, n: int, k: int, stack_size: int) -> dict:
 
 def fp64_peak(stream: Stream | None = None) -> float:
     return float(lib().libxstream_b200_fp64_peak(stream.handle if stream else None))
+
+
+def ozaki_gemm(transa: str, transb: str, M: int, N: int, K: int, alpha: float, a: DevBuf, lda: int, b: DevBuf,
+               ldb: int, beta: float, c: DevBuf, ldc: int, nslices: int = 8, trim: int = 0,
+               stream: Stream | None = None) -> int:
+    """libxstream_b200_ozaki_gemm: C = alpha*op(A)*op(B) + beta*C (column-major, device buffers)."""
+    return lib().libxstream_b200_ozaki_gemm(transa.encode(), transb.encode(), M, N, K, alpha, a.ptr, lda, b.ptr, ldb,
+                                            beta, c.ptr, ldc, nslices, trim, stream.handle if stream else None)

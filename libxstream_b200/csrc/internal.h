@@ -72,6 +72,16 @@ size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_sm
 int xs_launch_smm_f64(const int* dev_stack, int stack_size, const double* a, const double* b, double* c, int m, int n,
   int k, const xs_smm_params_t* params, void* scratch, size_t scratch_bytes, void* stream);
 
+/** Device address of the library's device error word (current device). */
+unsigned* xs_device_error_ptr(void);
+
+/** Ozaki scheme-1 FP64 GEMM on the int8 tensor cores (ozaki_gemm.cu): C = alpha*op(A)*op(B) + beta*C,
+    column-major, nslices in 1..8, slice pairs with sa + sb <= cutoff (cutoff < 0: all pairs).
+    scratch must hold xs_ozaki_gemm_scratch_bytes(). Returns a cudaError_t value. */
+size_t xs_ozaki_gemm_scratch_bytes(int M, int N, int K, int nslices);
+int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda, const double* b,
+  int ldb, double beta, double* c, int ldc, int nslices, int cutoff, void* scratch, size_t scratch_bytes, void* stream);
+
 /** Stable grouping of stacks by c (stack_sort.cu), one cooperative kernel for one stack or a batch:
     splits each AoS stack into keys (c) and payload (a | b << 32), resets the segment list, and
     writes each stack's grouped order to (kout, vout) at its offset off[s], using (k0, v0) and

@@ -19,7 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-/* Library-wide device error word: bit 0 = a grid barrier of the grouping sort timed out. */
+/* Library-wide device error word: bit 0 = a grid barrier of the grouping sort timed out, bit 2 = a
+   pipeline wait of the Ozaki GEMM timed out. */
 __device__ unsigned xs_device_error_word;
 
 namespace {
@@ -531,6 +532,19 @@ unsigned* xs_sort_queue_counter(void* sort_scratch, int which) {
 const unsigned* xs_sort_error_flag(void* sort_scratch) { return &((SortCtl*)sort_scratch)->err; }
 int xs_sort_launch_tiles(void) { return sort_grid_max() < kMaxGroupTiles ? sort_grid_max() : kMaxGroupTiles; }
 int xs_sort_tile_entries(int large) { return large ? kTileLarge : kTileSmall; }
+
+/* Device address of the error word for kernels of other translation units (one per device). */
+unsigned* xs_device_error_ptr(void) {
+  static unsigned* addr[64];
+  int dev = 0;
+  if (cudaSuccess != cudaGetDevice(&dev) || dev < 0 || dev >= 64) return NULL;
+  if (NULL == addr[dev]) {
+    void* p = NULL;
+    if (cudaSuccess != cudaGetSymbolAddress(&p, xs_device_error_word)) return NULL;
+    addr[dev] = (unsigned*)p;
+  }
+  return addr[dev];
+}
 
 int libxstream_b200_device_error(int reset) {
   unsigned e = 0;
