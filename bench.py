@@ -49,9 +49,12 @@ def parse_args():
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end arm (default: min(steps, 50))")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["stack23", "mixed", "mixed2m"], default="stack23",
+    p.add_argument("--workload", choices=["stack23", "mixed", "mixed2m", "gemm"], default="stack23",
                    help="stack23: the 23x23x23 stack (default); mixed / mixed2m: 12 mixed-shape stacks in one "
-                        "batch call replayed as a CUDA graph (stated sizes / scaled to 2M triples)")
+                        "batch call replayed as a CUDA graph (stated sizes / scaled to 2M triples); gemm: dense "
+                        "Ozaki int8 GEMM vs the plain FP64 DMMA GEMM")
+    p.add_argument("--gemm-sizes", default="2048,4096,8192,16384", help="square sizes of the gemm workload")
+    p.add_argument("--gemm-slices", default="5,6,7,8", help="slice counts of the gemm workload")
     return p.parse_args()
 
 
@@ -479,12 +482,118 @@ def run_mixed(args, d: Dist):
         print(json.dumps(line), flush=True)
 
 
+def run_gemm(args, d: Dist):
+    """Dense FP64 GEMM, square N: the Ozaki int8 tensor-core form for each slice count (all slice
+    pairs, and the triangle sa + sb <= s - 1) against the plain FP64 DMMA GEMM on the same inputs:
+    device time (CUDA events, L2 flushed between calls), FP64-equivalent TFLOP/s and the relative
+    max-norm error against the DMMA result (itself checked against numpy/BLAS at the smallest N).
+    Inputs: uniform[-1,1], and the same with row i of A scaled by 2^u, u uniform in [-30, 30]
+    (error per row relative to the row's largest entry)."""
+    import ctypes
+
+    import torch
+
+    import libxstream_b200 as xs
+
+    L = xs.lib()
+    xs.check(L.c_dbcsr_acc_init(), "init")
+    dev = torch.device("cuda", d.local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sizes = [int(x) for x in args.gemm_sizes.split(",") if x]
+    slices = [int(x) for x in args.gemm_slices.split(",") if x]
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
+    results = []
+    steps = max(1, min(args.steps, 10))
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            flush.zero_()
+            fn()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    gen = torch.Generator(device=dev)
+    for N in sizes:
+        gen.manual_seed(25071975 + N)
+        a = torch.rand(N * N, dtype=torch.float64, device=dev, generator=gen) * 2 - 1
+        b = torch.rand(N * N, dtype=torch.float64, device=dev, generator=gen) * 2 - 1
+        u = torch.randint(-30, 31, (N,), device=dev, generator=gen).to(torch.float64)
+        a_rs = (a.view(N, N) * torch.exp2(u)[None, :]).reshape(-1)  # column-major: row i of A is a[i::N]
+        c_ref = torch.empty(N * N, dtype=torch.float64, device=dev)
+        c = torch.empty_like(c_ref)
+        flops = 2.0 * N ** 3
+        for variant, av in (("uniform", a), ("row_scaled", a_rs)):
+            def plain():
+                xs.check(L.libxstream_b200_dgemm(b"N", b"N", N, N, N, 1.0, av.data_ptr(), N, b.data_ptr(), N, 0.0,
+                                                 c_ref.data_ptr(), N, sh), "dgemm")
+            ms_plain = timed(plain)
+            entry = {"N": N, "inputs": variant, "plain_dmma": {"ms": ms_plain, "tflops": flops / ms_plain * 1e-9}}
+            if N == sizes[0] and N <= 4096:
+                an = av.view(N, N).T.cpu().numpy()  # A as (row, col)
+                bn = b.view(N, N).T.cpu().numpy()
+                refn = an @ bn
+                got = c_ref.view(N, N).T.cpu().numpy()
+                entry["plain_dmma"]["relerr_vs_numpy"] = float(np.max(np.abs(got - refn)) / np.max(np.abs(refn)))
+            ref_rows = c_ref.view(N, N).abs().amax(dim=0)  # per-row max |C| (column-major view: dim 0 runs over columns)
+            ozk = []
+            for s in slices:
+                for label, trim in (("all_pairs", 0), ("triangle", s - 1)):
+                    def oz():
+                        xs.check(L.libxstream_b200_ozaki_gemm(b"N", b"N", N, N, N, 1.0, av.data_ptr(), N, b.data_ptr(), N,
+                                                              0.0, c.data_ptr(), N, s, trim, sh), "ozaki_gemm")
+                    ms = timed(oz)
+                    diff = (c - c_ref).view(N, N).abs()
+                    if variant == "uniform":
+                        err = float(diff.max() / c_ref.abs().max())
+                    else:
+                        err = float((diff.amax(dim=0) / ref_rows.clamp_min(1e-300)).max())
+                    cutoff = 2 * (s - 1) - trim
+                    npairs = sum(1 for x in range(s) for y in range(s) if x + y <= cutoff)
+                    ozk.append({"slices": s, "pairs": label, "npairs": npairs, "ms": ms,
+                                "tflops_fp64_equiv": flops / ms * 1e-9,
+                                "int8_tops": npairs * flops / ms * 1e-9, "relerr": err,
+                                "speedup_vs_plain": ms_plain / ms})
+            entry["ozaki"] = ozk
+            results.append(entry)
+        del a, b, a_rs, c, c_ref
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    best = None
+    for e in results:
+        for o in e["ozaki"]:
+            if o["relerr"] <= 1e-13 and (best is None or (e["N"], o["tflops_fp64_equiv"]) > (best[0], best[1]["tflops_fp64_equiv"])):
+                best = (e["N"], o, e["plain_dmma"]["tflops"])
+    line = {"metric": "dense FP64 GEMM TFLOP/s (FP64-equivalent), Ozaki int8 tensor-core form vs plain DMMA",
+            "value": best[1]["tflops_fp64_equiv"] if best else None, "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64 (int8 slices)",
+            "data": "synthetic", "config": {"workload": "square dense GEMM, N in " + args.gemm_sizes,
+                                            "l2": "flushed between timed calls"},
+            "best_at_1e-13": {"N": best[0], **best[1], "plain_tflops": best[2]} if best else None,
+            "results": results, "clocks": clocks}
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     d = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, d)
+        elif args.workload == "gemm":
+            run_gemm(args, d)
         elif args.workload != "stack23":
             run_mixed(args, d)
         else:

@@ -129,6 +129,14 @@ size_t libxstream_b200_process_scratch_bytes(int stack_size, int m, int n, int k
 int libxstream_b200_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
   const double* b, int ldb, double beta, double* c, int ldc, int nslices, int trim, void* stream);
 
+/**
+ * Plain FP64 GEMM on the FP64 tensor cores (DMMA): C = alpha*A*B + beta*C, column-major device
+ * operands, transa = transb = 'N' only (other values return nonzero). The baseline for
+ * libxstream_b200_ozaki_gemm; no counterpart in the reference (which compares with host DGEMM).
+ */
+int libxstream_b200_dgemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
+  const double* b, int ldb, double beta, double* c, int ldc, void* stream);
+
 #if defined(__cplusplus)
 }
 #endif

@@ -26,3 +26,13 @@ int libxstream_b200_ozaki_gemm(char transa, char transb, int M, int N, int K, do
   if (NULL != scratch) xs_scratch_free(scratch, stream);
   return xs_record_error(r, "ozaki_gemm");
 }
+
+int libxstream_b200_dgemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
+  const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
+  if (EXIT_SUCCESS != xs_smm_ensure_init()) return EXIT_FAILURE;
+  if (('N' != transa && 'n' != transa) || ('N' != transb && 'n' != transb)) {
+    return xs_record_error(1, "dgemm: only transa = transb = 'N'");
+  }
+  if (NULL == stream) stream = xs_default_stream();
+  return xs_record_error(xs_dgemm(M, N, K, alpha, a, lda, b, ldb, beta, c, ldc, stream), "dgemm");
+}

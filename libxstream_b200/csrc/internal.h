@@ -82,6 +82,10 @@ size_t xs_ozaki_gemm_scratch_bytes(int M, int N, int K, int nslices);
 int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda, const double* b,
   int ldb, double beta, double* c, int ldc, int nslices, int cutoff, void* scratch, size_t scratch_bytes, void* stream);
 
+/** Plain FP64 DMMA GEMM (dgemm.cu): C = alpha*A*B + beta*C, column-major, no transposes. */
+int xs_dgemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta, double* C,
+  int ldc, void* stream);
+
 /** Stable grouping of stacks by c (stack_sort.cu), one cooperative kernel for one stack or a batch:
     splits each AoS stack into keys (c) and payload (a | b << 32), resets the segment list, and
     writes each stack's grouped order to (kout, vout) at its offset off[s], using (k0, v0) and

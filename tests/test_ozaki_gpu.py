@@ -112,3 +112,23 @@ def test_long_k_runs_in_chunks(acc):
     c0 = g.uniform(-1, 1, size=(M, N))
     got = run(A, stream, "N", "N", M, N, K, a, b, c0, nslices=8)
     assert relerr(got, c0 + a @ b) <= 1e-14
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 16), (200, 300, 130), (129, 257, 1001), (64, 40, 7)])
+def test_plain_dgemm_matches_fp64(acc, shape):
+    """The plain FP64 DMMA GEMM (the comparison baseline) against numpy/BLAS FP64."""
+    A, stream = acc
+    M, N, K = shape
+    g = W.rng(4242 + K)
+    a = g.uniform(-1, 1, size=(M, K))
+    b = g.uniform(-1, 1, size=(K, N))
+    c0 = g.uniform(-1, 1, size=(M, N))
+    da = A.DevBuf.from_array(a.ravel(order="F"), stream)
+    db = A.DevBuf.from_array(b.ravel(order="F"), stream)
+    dc = A.DevBuf.from_array(c0.ravel(order="F"), stream)
+    assert A.dgemm(M, N, K, 0.5, da, M, db, K, -2.0, dc, M, stream) == 0
+    got = dc.download(np.zeros(M * N), stream).reshape((M, N), order="F")
+    stream.sync()
+    assert relerr(got, 0.5 * (a @ b) - 2.0 * c0) <= 1e-14
+    for buf in (da, db, dc):
+        buf.free()
