@@ -49,10 +49,13 @@ def parse_args():
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end arm (default: min(steps, 50))")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["stack23", "mixed", "mixed2m", "gemm"], default="stack23",
+    p.add_argument("--workload", choices=["stack23", "mixed", "mixed2m", "gemm", "ozaki"], default="stack23",
                    help="stack23: the 23x23x23 stack (default); mixed / mixed2m: 12 mixed-shape stacks in one "
                         "batch call replayed as a CUDA graph (stated sizes / scaled to 2M triples); gemm: dense "
-                        "Ozaki int8 GEMM vs the plain FP64 DMMA GEMM")
+                        "Ozaki int8 GEMM vs the plain FP64 DMMA GEMM; ozaki: Ozaki int8 stack form vs the plain "
+                        "stack path on 32^3/45^3/64^3 stacks with exponent-spread entries")
+    p.add_argument("--ozaki-shapes", default="32,45,64", help="cube block sizes of the ozaki workload")
+    p.add_argument("--ozaki-stack", type=int, default=200000, help="triples per stack of the ozaki workload")
     p.add_argument("--gemm-sizes", default="2048,4096,8192,16384", help="square sizes of the gemm workload")
     p.add_argument("--gemm-slices", default="5,6,7,8", help="slice counts of the gemm workload")
     return p.parse_args()
@@ -586,6 +589,124 @@ def run_gemm(args, d: Dist):
         print(json.dumps(line), flush=True)
 
 
+def run_ozaki_smm(args, d: Dist):
+    """Ozaki int8 stack form against the plain FP64 stack path on the same stacks: cube blocks of
+    the given sizes, S triples, A/B pools of 8192 blocks, C pool of 2048 blocks, entries mantissa
+    U[1,2) x 2^e, e uniform in [-20, 20], random sign; a/b uniform, c Zipf(1.1). Per slice count:
+    device time per call (CUDA events, L2 flushed), FP64-equivalent GFLOP/s and the relative
+    max-norm error per C block against the plain path's FP64 result (itself checked against the
+    CPU oracle)."""
+    import ctypes
+
+    import libxstream_b200 as xs
+    import oracle
+    from libxstream_b200 import acc as A
+    from libxstream_b200 import workloads as W
+
+    L = xs.lib()
+    A.init()
+    stream = A.Stream("bench")
+    flush = A.DevBuf(FLUSH_BYTES)
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
+    steps = max(1, min(args.steps, 20))
+    ev = []
+    for _ in range(2 * steps):
+        e = ctypes.c_void_p()
+        xs.check(L.libxstream_b200_event_create_timed(ctypes.byref(e)), "event")
+        ev.append(e.value)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            flush.zero(stream)
+            fn()
+        stream.sync()
+        for i in range(steps):
+            flush.zero(stream)
+            L.c_dbcsr_acc_event_record(ev[2 * i], stream.handle)
+            fn()
+            L.c_dbcsr_acc_event_record(ev[2 * i + 1], stream.handle)
+        stream.sync()
+        return sum(L.libxstream_b200_event_elapsed_ms(ev[2 * i], ev[2 * i + 1]) for i in range(steps)) / steps
+
+    def kernel_breakdown(fn, names):
+        L.libxstream_b200_profile_reset()
+        L.libxstream_b200_profile_enable(1)
+        flush.zero(stream)
+        fn()
+        stream.sync()
+        L.libxstream_b200_profile_enable(0)
+        out = {}
+        for name in names:
+            nl, ms, gf, gb = ctypes.c_long(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            if L.libxstream_b200_profile_query(name.encode(), ctypes.byref(nl), ctypes.byref(ms), ctypes.byref(gf),
+                                               ctypes.byref(gb)) == 0 and nl.value > 0:
+                out[name] = round(ms.value, 4)
+        return out
+
+    results = []
+    for size in [int(x) for x in args.ozaki_shapes.split(",") if x]:
+        m = n = k = size
+        S = args.ozaki_stack
+        case = W.stack_case(m, n, k, S, 8192, 8192, 2048, seed=25071975 + size, values="spread")
+        da, db = A.DevBuf.from_array(case.a, stream), A.DevBuf.from_array(case.b_rowmajor(), stream)
+        ds = A.DevBuf.from_array(case.stack, stream)
+        dc = A.DevBuf(case.nc * m * n * 8)
+        flops = case.flops
+
+        def plain():
+            xs.check(A.process(ds, S, da, db, dc, m, n, k, stream), "process")
+        ms_plain = timed(plain)
+        prof_plain = kernel_breakdown(plain, ("sort", "smm", "combine"))
+        dc.zero(stream)
+        plain()
+        ref = dc.download(np.zeros(case.nc * m * n), stream)
+        stream.sync()
+        entry = {"m": m, "n": n, "k": k, "stack": S, "gflop": flops * 1e-9,
+                 "plain": {"ms": ms_plain, "gflops": flops / ms_plain * 1e-6, "kernels_ms": prof_plain}}
+        if size == int(args.ozaki_shapes.split(",")[0]):
+            cpu = np.zeros_like(ref)
+            oracle.smm_fast(case.stack, case.a, case.b, cpu, m, n, k)
+            entry["plain"]["relerr_vs_cpu_oracle"] = oracle.block_relerr(ref, cpu, m * n)
+        oz = []
+        for ns, trim in ((3, 2), (4, 3), (5, 4), (6, 5), (7, 6), (8, 7), (8, 0)):
+            def ozaki():
+                xs.check(A.process_ozaki(ds, S, m, n, k, da, case.na, db, case.nb, dc, ns, trim, stream), "process_ozaki")
+            ms = timed(ozaki)
+            dc.zero(stream)
+            ozaki()
+            got = dc.download(np.zeros(case.nc * m * n), stream)
+            stream.sync()
+            cutoff = 2 * (ns - 1) - trim
+            o = {"slices": ns, "pairs": "triangle" if trim == ns - 1 else ("all" if trim == 0 else f"cutoff {cutoff}"),
+                 "ms": ms, "gflops": flops / ms * 1e-6, "speedup_vs_plain": ms_plain / ms,
+                 "relerr": oracle.block_relerr(got, ref, m * n)}
+            if ns == 7:
+                o["kernels_ms"] = kernel_breakdown(ozaki, ("ozaki_slice_pools", "sort", "ozaki_smm", "ozaki_combine"))
+            oz.append(o)
+        entry["ozaki"] = oz
+        results.append(entry)
+        for b in (da, db, ds, dc):
+            b.free()
+    clocks = sampler.stop()
+    for e in ev:
+        L.c_dbcsr_acc_event_destroy(e)
+    flush.free()
+    stream.destroy()
+    best = [max((o for o in e["ozaki"] if o["relerr"] <= 1e-13), key=lambda o: o["gflops"], default=None) for e in results]
+    line = {"metric": METRIC, "value": None if None in best else min(b["speedup_vs_plain"] for b in best),
+            "unit": "x (Ozaki at <=1e-13 over plain, worst shape)", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64 (int8 slices)", "data": "synthetic",
+            "config": {"workload": f"Ozaki int8 stack form vs plain FP64 stack path, cubes {args.ozaki_shapes}, "
+                                   f"{args.ozaki_stack} triples, A/B pools 8192 blocks, C pool 2048 blocks, "
+                                   "entries U[1,2)*2^U{-20..20} random sign, c Zipf(1.1)",
+                       "l2": "flushed between timed calls (256 MiB memset, outside the timed events)"},
+            "best_at_1e-13": [{"m": e["m"], **b} if b else None for e, b in zip(results, best)],
+            "results": results, "clocks": clocks}
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     d = Dist()
@@ -594,6 +715,8 @@ def main():
             run_reference(args, d)
         elif args.workload == "gemm":
             run_gemm(args, d)
+        elif args.workload == "ozaki":
+            run_ozaki_smm(args, d)
         elif args.workload != "stack23":
             run_mixed(args, d)
         else:

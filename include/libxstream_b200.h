@@ -137,6 +137,20 @@ int libxstream_b200_ozaki_gemm(char transa, char transb, int M, int N, int K, do
 int libxstream_b200_dgemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
   const double* b, int ldb, double beta, double* c, int ldc, void* stream);
 
+/**
+ * Ozaki scheme-1 form of libsmm_acc_process for FP64 stacks of one shape with m, n, k <= 64:
+ * C[c] += A[a]*B[b] with every block row of A / column of B split into nslices (1..8; <= 0 means 7)
+ * int8 digit slices under its own power-of-two scale and the slice pairs with
+ * sa + sb <= 2*(nslices-1) - trim multiplied on the int8 tensor cores (exact int32 sums), then
+ * recombined and accumulated in FP64. Same data contract as libsmm_acc_process (1-based offsets,
+ * B pool already transposed to k x n row-major), plus the pool sizes na, nb in blocks; every offset
+ * must be a multiple of the block size (otherwise bit 3 of libxstream_b200_device_error is set).
+ * Returns -1 for shapes it does not handle (use libsmm_acc_process), 0 on success. No counterpart in
+ * the reference, whose Ozaki code is dense GEMM only (samples/ozaki).
+ */
+int libxstream_b200_process_ozaki(const int* dev_param_stack, int stack_size, int m, int n, int k, const double* dev_a,
+  int na, const double* dev_b, int nb, double* dev_c, int nslices, int trim, void* stream);
+
 #if defined(__cplusplus)
 }
 #endif

@@ -171,3 +171,10 @@ def dgemm(M: int, N: int, K: int, alpha: float, a: DevBuf, lda: int, b: DevBuf, 
     """libxstream_b200_dgemm (plain FP64 DMMA GEMM, 'N', 'N')."""
     return lib().libxstream_b200_dgemm(b"N", b"N", M, N, K, alpha, a.ptr, lda, b.ptr, ldb, beta, c.ptr, ldc,
                                        stream.handle if stream else None)
+
+
+def process_ozaki(stack: DevBuf, stack_size: int, m: int, n: int, k: int, a: DevBuf, na: int, b: DevBuf, nb: int,
+                  c: DevBuf, nslices: int = 7, trim: int = 0, stream: Stream | None = None) -> int:
+    """libxstream_b200_process_ozaki (B pool already transposed to k x n row-major)."""
+    return lib().libxstream_b200_process_ozaki(stack.ptr, stack_size, m, n, k, a.ptr, na, b.ptr, nb, c.ptr, nslices, trim,
+                                               stream.handle if stream else None)

@@ -36,3 +36,24 @@ int libxstream_b200_dgemm(char transa, char transb, int M, int N, int K, double 
   if (NULL == stream) stream = xs_default_stream();
   return xs_record_error(xs_dgemm(M, N, K, alpha, a, lda, b, ldb, beta, c, ldc, stream), "dgemm");
 }
+
+int libxstream_b200_process_ozaki(const int* dev_param_stack, int stack_size, int m, int n, int k, const double* dev_a,
+  int na, const double* dev_b, int nb, double* dev_c, int nslices, int trim, void* stream) {
+  void* scratch = NULL;
+  size_t nbytes;
+  int r, cutoff;
+  if (0 >= stack_size) return EXIT_SUCCESS;
+  if (m < 1 || n < 1 || k < 1 || m > 64 || n > 64 || k > 64) return -1; /* not handled: use the plain path */
+  if (EXIT_SUCCESS != xs_smm_ensure_init()) return EXIT_FAILURE;
+  if (NULL == stream) stream = xs_default_stream();
+  if (0 >= nslices) nslices = 7;
+  if (8 < nslices || 1 > na || 1 > nb) return xs_record_error(1, "process_ozaki: invalid arguments");
+  cutoff = 2 * (nslices - 1) - (0 < trim ? trim : 0);
+  if (0 > cutoff) cutoff = 0;
+  nbytes = xs_smm_ozaki_scratch_bytes(stack_size, m, n, k, na, nb, nslices);
+  if (0 == nbytes || EXIT_SUCCESS != xs_scratch_alloc(&scratch, nbytes, stream)) return EXIT_FAILURE;
+  r = xs_launch_smm_ozaki(dev_param_stack, stack_size, m, n, k, dev_a, na, dev_b, nb, dev_c, nslices, cutoff, scratch, nbytes,
+    stream);
+  xs_scratch_free(scratch, stream);
+  return xs_record_error(r, "process_ozaki");
+}

@@ -82,6 +82,13 @@ size_t xs_ozaki_gemm_scratch_bytes(int M, int N, int K, int nslices);
 int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda, const double* b,
   int ldb, double beta, double* c, int ldc, int nslices, int cutoff, void* scratch, size_t scratch_bytes, void* stream);
 
+/** Ozaki scheme-1 stack multiply (ozaki_smm.cu): C[c] += A[a]*B[b] for one shape m, n, k <= 64 with
+    int8 tensor-core slice products; A pool of na m x k column-major blocks, B pool of nb k x n
+    row-major blocks, 1-based block-aligned offsets. Returns a cudaError_t value. */
+size_t xs_smm_ozaki_scratch_bytes(int S, int m, int n, int k, int na, int nb, int nslices);
+int xs_launch_smm_ozaki(const int* dev_stack, int S, int m, int n, int k, const double* a, int na, const double* b, int nb,
+  double* c, int nslices, int cutoff, void* scratch, size_t scratch_bytes, void* stream);
+
 /** Plain FP64 DMMA GEMM (dgemm.cu): C = alpha*A*B + beta*C, column-major, no transposes. */
 int xs_dgemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta, double* C,
   int ldc, void* stream);

@@ -31,6 +31,7 @@
  */
 #include "internal.h"
 #include "tc_ptx.cuh"
+#include "ozaki_digits.cuh"
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>
@@ -40,6 +41,7 @@ extern "C" unsigned* xs_device_error_ptr(void);
 
 namespace {
 using namespace xs_tc;
+using namespace xs_oz;
 
 constexpr int kBM = 128, kBN = 256, kBK = 128, kStages = 4;
 constexpr int kMaxSlices = 8;
@@ -51,30 +53,6 @@ constexpr int kGemmThreads = 192;
 constexpr unsigned kErrOzakiTimeout = 4u; /* device error word bit: an Ozaki pipeline wait timed out */
 
 /* ------------------------------------------------------------------------------ slicing */
-
-/* IEEE-754 split: sign, biased exponent, significand with the implicit bit; zero, subnormal, Inf
-   and NaN give exponent 0 and significand 0 (ozaki_common.cl:789-806). */
-__device__ __forceinline__ void ieee_split(double v, unsigned& sign, int& bexp, unsigned long long& mant) {
-  const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
-  sign = (unsigned)(bits >> 63);
-  bexp = (int)((bits >> 52) & 2047u);
-  mant = (bits & 0x000FFFFFFFFFFFFFull) | 0x0010000000000000ull;
-  if (0 == bexp || 2047 == bexp) {
-    bexp = 0;
-    mant = 0;
-  }
-}
-
-__device__ __forceinline__ int biased_exp(double v) {
-  const int e = (int)(((unsigned long long)__double_as_longlong(v) >> 52) & 2047u);
-  return (2047 == e) ? 0 : e;
-}
-
-/* Digit s (0..7) of an aligned significand, signed; digit 7 carries bits [0,3] times 8. */
-__device__ __forceinline__ int slice_digit(unsigned long long aligned, unsigned sign, int s) {
-  const int d = (s < 7) ? (int)((aligned >> (46 - 7 * s)) & 127u) : (int)((aligned & 15u) << 3);
-  return sign ? -d : d;
-}
 
 /* Row maxima of the biased exponent, rows contiguous in memory: element (r, k) at x[r + k*ld].
    Grid (ceil(R/256), k-chunks); partial maxima meet in emax[] (zeroed by the caller) by atomicMax. */

@@ -749,19 +749,6 @@ struct BatchPlan {
   size_t total;
 };
 
-int pick_tiles_dim(int dim) { /* least padded split of ceil(dim/8) fragments into sub-tiles of <= 4 */
-  const int frags = (dim + 7) / 8;
-  int best = 1, bestwaste = 1 << 30;
-  for (int t = 4; t >= 1; --t) {
-    const int waste = (frags + t - 1) / t * t - frags;
-    if (waste < bestwaste) {
-      bestwaste = waste;
-      best = t;
-    }
-  }
-  return best;
-}
-
 /* Work decomposition of a batch: stacks split into parts of at most xs_stack_group_max() entries;
    per part a tile class (MT x NT from the parameter table) and a chunk length L chosen so that every
    work item (W chunks x one sub-tile) costs about the same, ~4 items per resident CTA. */

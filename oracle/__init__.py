@@ -39,6 +39,8 @@ def lib() -> ctypes.CDLL:
                                             ctypes.POINTER(ctypes.c_byte), _ip]
         _lib.oracle_ozaki_gemm.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int]
+        _lib.oracle_ozaki_smm.argtypes = [_ip, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _lib.oracle_slice_low_bit.argtypes = [ctypes.c_int]
         _lib.oracle_slice_low_bit.restype = ctypes.c_int
     return _lib
@@ -118,5 +120,14 @@ def ozaki_gemm(A: np.ndarray, B: np.ndarray, C: np.ndarray, M: int, N: int, K: i
     return C
 
 
-__all__ = ["lib", "smm", "smm_fast", "transpose", "norms", "block_relerr", "max_threads", "ozaki_slice", "ozaki_gemm", "OUT",
+def ozaki_smm(stack: np.ndarray, a: np.ndarray, b: np.ndarray, c: np.ndarray, m: int, n: int, k: int, nslices: int,
+              cutoff: int = -1, b_rowmajor: bool = True) -> np.ndarray:
+    """Ozaki scheme-1 stack multiply (per-block row/column scaling) C += A*B in place; returns c."""
+    stack = np.ascontiguousarray(stack, dtype=np.int32)
+    lib().oracle_ozaki_smm(_p(stack, ctypes.c_int), stack.size // 3, _p(a, ctypes.c_double), _p(b, ctypes.c_double),
+                           _p(c, ctypes.c_double), m, n, k, int(b_rowmajor), nslices, cutoff)
+    return c
+
+
+__all__ = ["lib", "smm", "smm_fast", "transpose", "norms", "block_relerr", "max_threads", "ozaki_slice", "ozaki_gemm", "ozaki_smm", "OUT",
            "Path"]

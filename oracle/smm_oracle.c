@@ -310,3 +310,53 @@ done:
   free(ea);
   free(eb);
 }
+
+/* Ozaki scheme-1 stack multiply: for every entry, C[c] += A[a] * B[b] where each row of the A block
+   and each column of the B block is sliced with its own row / column exponent (the rule of
+   oracle_ozaki_slice applied per block), all slice pairs with sa + sb <= cutoff are multiplied in
+   int64 and scaled and accumulated in FP64 in (sa, sb) order, per entry in stack order. B blocks
+   are k x n row-major when b_rowmajor (the device layout after libsmm_acc_transpose), else
+   column-major. */
+void oracle_ozaki_smm(const int* stack, int S, const double* a, const double* b, double* c, int m, int n, int k,
+  int b_rowmajor, int nslices, int cutoff) {
+  signed char* const da = (signed char*)malloc((size_t)nslices * m * k);
+  signed char* const db = (signed char*)malloc((size_t)nslices * n * k);
+  double* const blk = (double*)malloc(sizeof(double) * (size_t)m * n);
+  int* const ea = (int*)malloc(sizeof(int) * (size_t)m);
+  int* const eb = (int*)malloc(sizeof(int) * (size_t)n);
+  int e, i, j, kk, sa, sb;
+  if (NULL == da || NULL == db || NULL == blk || NULL == ea || NULL == eb) goto done;
+  for (e = 0; e < S; ++e) {
+    const double* const A = a + stack[3 * e + 0] - 1;
+    const double* const B = b + stack[3 * e + 1] - 1;
+    double* const C = c + stack[3 * e + 2] - 1;
+    oracle_ozaki_slice(A, m, k, 1, m, nslices, da, ea);
+    if (b_rowmajor) oracle_ozaki_slice(B, n, k, 1, n, nslices, db, eb); /* column j: element kk at kk*n + j */
+    else oracle_ozaki_slice(B, n, k, k, 1, nslices, db, eb);            /* column j: element kk at kk + j*k */
+    for (j = 0; j < n; ++j) {
+      for (i = 0; i < m; ++i) {
+        double acc = 0.0;
+        if (0 != ea[i] && 0 != eb[j]) {
+          for (sa = 0; sa < nslices; ++sa) {
+            for (sb = 0; sb < nslices; ++sb) {
+              int64_t dot = 0;
+              if (0 <= cutoff && sa + sb > cutoff) continue;
+              for (kk = 0; kk < k; ++kk) {
+                dot += (int64_t)da[((size_t)sa * m + i) * k + kk] * (int64_t)db[((size_t)sb * n + j) * k + kk];
+              }
+              acc += ldexp((double)dot, oracle_slice_low_bit(sa) + oracle_slice_low_bit(sb) - 104 + (ea[i] - 1023) + (eb[j] - 1023));
+            }
+          }
+        }
+        blk[(size_t)j * m + i] = acc;
+      }
+    }
+    for (i = 0; i < m * n; ++i) C[i] += blk[i];
+  }
+done:
+  free(da);
+  free(db);
+  free(blk);
+  free(ea);
+  free(eb);
+}
