@@ -151,6 +151,56 @@ int libxstream_b200_dgemm(char transa, char transb, int M, int N, int K, double 
 int libxstream_b200_process_ozaki(const int* dev_param_stack, int stack_size, int m, int n, int k, const double* dev_a,
   int na, const double* dev_b, int nb, double* dev_c, int nslices, int trim, void* stream);
 
+/**
+ * Exhaustive autotuner of the plain stack kernel (replaces samples/smm/tune_multiply.py's OpenTuner
+ * search; the space here is the precompiled tile classes). libxstream_b200_tune_candidates writes
+ * the (mt, nt, kp) triples tried for (m, n) and returns their count; libxstream_b200_tune times each
+ * on synthetic data of the given shape and stack size (reps calls after one warm-up; seed fixes the
+ * data) and, with ozaki_slices > 0 and m, n, k <= 64, the Ozaki form last; ms_out receives the
+ * milliseconds per call. Returns the number of times written, < 0 on error. Synchronous.
+ */
+int libxstream_b200_tune_candidates(int m, int n, int* mt_nt_kp, int capacity);
+int libxstream_b200_tune(int m, int n, int k, int stack_size, int reps, int ozaki_slices, unsigned seed, float* ms_out,
+  int capacity, void* stream);
+
+/**
+ * Learned parameter predictor: 3-layer FP32 MLP (width 64) from (m, n, k, stack size, exponent
+ * spread) to the best of the 32 tile classes (c = (mt-1)*8 + (nt-1)*2 + (kp==4)) and to the
+ * plain-vs-Ozaki choice. Samples are raw int quintuples (m, n, k, S, spread); r[N][32] holds each
+ * configuration's time divided by the best (0 = not applicable), z[N] is 1 when the Ozaki form was
+ * faster, 0 when not, -1 when unmeasured. Training (Adam, device kernels) updates weights in place
+ * and records the mean loss per step; grad/forward expose one pass for checking; predict runs the
+ * inference kernel; install builds the lookup table used by libsmm_acc_process for shapes without
+ * a tuned record (LIBXSTREAM_B200_MLP=<file> installs one at init). No counterpart in the reference
+ * beyond its use of LIBXS predict models (samples/smm/tune_multiply.py).
+ */
+int libxstream_b200_mlp_nweights(void);
+int libxstream_b200_mlp_train(const int* raw, const float* r, const float* z, int n, int steps, float lr, float* weights,
+  float* loss_hist);
+int libxstream_b200_mlp_grad(const float* weights, const int* raw, const float* r, const float* z, int n, float* grad,
+  float* loss);
+int libxstream_b200_mlp_forward(const float* weights, const int* raw, int n, float* y);
+int libxstream_b200_mlp_predict(const float* weights, const int* raw, int n, unsigned char* config, float* confidence,
+  float* p_ozaki);
+int libxstream_b200_mlp_install(const float* weights, int nweights);
+int libxstream_b200_mlp_lookup(int m, int n, int k, int stack_size, int* mt_nt_kp, float* confidence);
+
+/**
+ * DBM interplay (samples/smm/smm_acc_opencl.h:114-118). libxstream_b200_dbm_launch_fn_t is the
+ * reference's opencl_libsmm_acc_dbm_launch_fn_t: ntasks records, param_format = m | n << 8 | k << 16
+ * for one shape (0: mixed shapes). libxstream_b200_set_dbm_launch_fn replaces
+ * opencl_libsmm_acc_set_dbm_launch_fn: once set (non-NULL), libsmm_acc_process hands FP64 stacks of
+ * one shape to that function with alpha = 1. libxstream_b200_dbm_launch runs such a batch with this
+ * library's stack kernels -- 6-int records (m, n, k, a, b, c), 0-based offsets, C += alpha*A*B,
+ * layouts as for libsmm_acc_process -- the reuse of LIBSMM kernels by DBM that
+ * opencl_libsmm_acc_process(..., param_format) offers (smm_kernel.c:82-88); mixed shapes return -1.
+ */
+typedef int (*libxstream_b200_dbm_launch_fn_t)(void* stream, double alpha, int ntasks, int param_format, const int* params_host,
+  const int* params, const double* pack_a_data, const double* pack_b_data, double* shard_c_data);
+void libxstream_b200_set_dbm_launch_fn(libxstream_b200_dbm_launch_fn_t launch_fn);
+int libxstream_b200_dbm_launch(void* stream, double alpha, int ntasks, int param_format, const int* params_host,
+  const int* params, const double* pack_a_data, const double* pack_b_data, double* shard_c_data);
+
 #if defined(__cplusplus)
 }
 #endif

@@ -22,8 +22,8 @@ OBJ_DIR = PKG / "_build"
 LIB = OUT_DIR / "libxstream_b200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-C_SOURCES = ["acc_runtime.c", "smm_params.c", "smm_acc.c", "profile.c", "gemm_api.c"]
-CU_SOURCES = ["smm_kernels.cu", "stack_sort.cu", "smm_noalloc.cu", "ozaki_gemm.cu", "dgemm.cu", "ozaki_smm.cu"]
+C_SOURCES = ["acc_runtime.c", "smm_params.c", "smm_acc.c", "profile.c", "gemm_api.c", "predictor.c"]
+CU_SOURCES = ["smm_kernels.cu", "stack_sort.cu", "smm_noalloc.cu", "ozaki_gemm.cu", "dgemm.cu", "ozaki_smm.cu", "tune.cu", "mlp.cu"]
 
 
 def _nvcc() -> str:
@@ -78,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             sys.stderr.write(" ".join(cmd) + "\n" + out)
             raise RuntimeError(f"nvcc failed on {cmd[-3]}")
     tmp = LIB.with_suffix(".so.tmp")
-    _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lpthread"])
+    _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lpthread", "-ldl"])
     os.replace(tmp, LIB)
     return LIB
 

@@ -57,6 +57,18 @@ typedef struct xs_smm_params_t {
   int sorted;  /* 1: the stack is known to be grouped by c (skip the device sort) */
 } xs_smm_params_t;
 
+/** Where a lookup's parameters came from. */
+#define XS_PARAMS_DEFAULT 0   /* default heuristic */
+#define XS_PARAMS_TUNED 1     /* tuned record (table / CSV / autotuner) */
+#define XS_PARAMS_PREDICTED 2 /* learned predictor */
+#define XS_PARAMS_LOWCONF 3   /* predictor below its confidence threshold (its prediction is used) */
+void xs_params_lookup_ex(int type, int m, int n, int k, int stack_size, xs_smm_params_t* out, int* source);
+/** Runs the exhaustive tuner for (m, n, k, stack_size) and records the best configuration when
+    LIBXSTREAM_B200_AUTOTUNE=1, no tuned record exists, the predictor is absent or not confident,
+    and the stream is not being captured. */
+void xs_autotune_if_needed(int m, int n, int k, int stack_size, void* stream);
+int xs_mlp_load_file(const char* path);
+
 /** Shape-specialised kernels compiled for (m, n, k): writes up to capacity (mt, nt, kp) triples,
     returns how many exist. */
 int xs_smm_f64_specialized(int m, int n, int k, int* mt_nt_kp, int capacity);
@@ -71,6 +83,10 @@ size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_sm
  */
 int xs_launch_smm_f64(const int* dev_stack, int stack_size, const double* a, const double* b, double* c, int m, int n,
   int k, const xs_smm_params_t* params, void* scratch, size_t scratch_bytes, void* stream);
+/** Same with C += alpha*A*B and the stack in parameter format `format` (0: 1-based (a, b, c) triples;
+    otherwise 6-int records whose 0-based (a, b, c) offsets sit at +3, the DBM task layout). */
+int xs_launch_smm_f64_ex(const int* dev_stack, int stack_size, int format, double alpha, const double* a, const double* b,
+  double* c, int m, int n, int k, const xs_smm_params_t* params, void* scratch, size_t scratch_bytes, void* stream);
 
 /** Device address of the library's device error word (current device). */
 unsigned* xs_device_error_ptr(void);
@@ -89,6 +105,22 @@ size_t xs_smm_ozaki_scratch_bytes(int S, int m, int n, int k, int na, int nb, in
 int xs_launch_smm_ozaki(const int* dev_stack, int S, int m, int n, int k, const double* a, int na, const double* b, int nb,
   double* c, int nslices, int cutoff, void* scratch, size_t scratch_bytes, void* stream);
 
+/** Exhaustive autotuner (tune.cu): candidate (mt, nt, kp) triples of the plain kernel for (m, n),
+    and the time per call of each (plus the Ozaki form with ozaki_slices > 0) on synthetic data. */
+int xs_tune_candidates(int m, int n, int* mt_nt_kp, int cap);
+int xs_tune(int m, int n, int k, int S, int reps, int ozaki_slices, unsigned seed, float* ms_out, int cap, void* stream);
+
+/** Learned parameter predictor (mlp.cu): 3-layer FP32 MLP, raw inputs (m, n, k, S, spread) per sample,
+    r[N][32] time ratios (0 = configuration not applicable), z[N] Ozaki label (1, 0, or -1 unknown). */
+int xs_mlp_nweights(void);
+int xs_mlp_train(const int* raw, const float* r, const float* z, int N, int steps, float lr, float* weights, float* loss_hist);
+int xs_mlp_grad(const float* weights, const int* raw, const float* r, const float* z, int N, float* grad, float* loss);
+int xs_mlp_forward(const float* weights, const int* raw, int N, float* y);
+int xs_mlp_predict(const float* weights, const int* raw, int N, unsigned char* cfg, float* conf, float* pz);
+int xs_mlp_install(const float* weights);
+void xs_mlp_uninstall(void);
+int xs_mlp_lookup(int m, int n, int k, int S, int* mt, int* nt, int* kp, float* confidence);
+
 /** Plain FP64 DMMA GEMM (dgemm.cu): C = alpha*A*B + beta*C, column-major, no transposes. */
 int xs_dgemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta, double* C,
   int ldc, void* stream);
@@ -103,6 +135,7 @@ typedef struct xs_sort_batch_t {
   int nstacks;
   int gidx[XS_MAX_BATCH];       /* index of the stack within the call (statistics slot) */
   const int* stack[XS_MAX_BATCH];
+  int format[XS_MAX_BATCH];     /* 0: (a, b, c) triples of 1-based offsets; else 6-int records, 0-based (a, b, c) at +3 */
   int S[XS_MAX_BATCH];          /* entries per stack (>= 1) */
   int off[XS_MAX_BATCH];        /* first output position of each stack */
   int tile_begin[XS_MAX_BATCH]; /* filled by the launcher */
@@ -123,6 +156,8 @@ int xs_stack_group_fits(const xs_sort_batch_t* desc);
 /** Grouping of a batch that fits one launch; the control block must have been cleared for the call
     (xs_sort_clear_ctl) before the first launch of the call. */
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
+int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
 int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);

@@ -21,7 +21,10 @@
 #include "internal.h"
 #include "../../include/libsmm_acc.h"
 #include "../../include/libxstream_b200.h"
+#include <dlfcn.h>
 #include <pthread.h>
+#include <string.h>
+#include <unistd.h>
 #include <stdio.h>
 #include <stdlib.h>
 
@@ -42,6 +45,27 @@ int libsmm_acc_init(void) {
   }
   if (EXIT_SUCCESS == result) ++xs_smm_initialized;
   pthread_mutex_unlock(&xs_smm_lock);
+  if (EXIT_SUCCESS == result && 1 == xs_smm_initialized) { /* learned predictor */
+    const char* const mlp = getenv("LIBXSTREAM_B200_MLP");
+    if (NULL != mlp && '\0' != *mlp) {
+      if ('0' != *mlp && EXIT_SUCCESS == xs_ensure_device() && EXIT_SUCCESS != xs_mlp_load_file(mlp)) {
+        fprintf(stderr, "WARNING LIBSMM/B200: cannot load predictor \"%s\"\n", mlp);
+      }
+    }
+    else { /* the predictor shipped next to the library: <dir of the .so>/../params/mlp_b200.txt */
+      Dl_info info;
+      if (0 != dladdr((void*)&libsmm_acc_init, &info) && NULL != info.dli_fname) {
+        char path[4096];
+        const char* const slash = strrchr(info.dli_fname, '/');
+        const int dirlen = (NULL != slash) ? (int)(slash - info.dli_fname) : 1;
+        snprintf(path, sizeof(path), "%.*s/../params/mlp_b200.txt", dirlen, NULL != slash ? info.dli_fname : ".");
+        if (0 == access(path, R_OK) && EXIT_SUCCESS == xs_ensure_device() && EXIT_SUCCESS == xs_mlp_load_file(path) &&
+            2 <= xs_verbosity()) {
+          fprintf(stderr, "INFO LIBSMM/B200: predictor %s\n", path);
+        }
+      }
+    }
+  }
   return result;
 }
 
@@ -75,16 +99,51 @@ int libxstream_b200_process_suitable(
   return (dbcsr_type_real_8 == datatype) ? 1 : 0;
 }
 
+static int xs_process_format(const int* dev_param_stack, int stack_size, int format, double alpha, libsmm_acc_data_t datatype,
+  const void* dev_a_data, const void* dev_b_data, void* dev_c_data, int m_max, int n_max, int k_max, int max_kernel_dim,
+  c_dbcsr_acc_bool_t def_mnk, void* stack_stream);
+
+/* DBM launch hook (samples/smm/smm_kernel.c:71-76, smm_acc.c:579-585): when set, FP64 stacks of one
+   shape go to the caller's kernel with the shape packed as m | n << 8 | k << 16. */
+static libxstream_b200_dbm_launch_fn_t xs_dbm_launch_fn = NULL;
+
+void libxstream_b200_set_dbm_launch_fn(libxstream_b200_dbm_launch_fn_t launch_fn) { xs_dbm_launch_fn = launch_fn; }
+
 int libsmm_acc_process(const int* host_param_stack, const int* dev_param_stack, int stack_size, libsmm_acc_data_t datatype,
   const void* dev_a_data, const void* dev_b_data, void* dev_c_data, int m_max, int n_max, int k_max, int max_kernel_dim,
   c_dbcsr_acc_bool_t def_mnk, void* stack_stream, void* c_stream) {
+  if (NULL != xs_dbm_launch_fn && dbcsr_type_real_8 == datatype && 0 != def_mnk && 0 < stack_size && m_max < 128 && n_max < 128 &&
+      k_max < 128) {
+    return xs_dbm_launch_fn(stack_stream, 1.0, stack_size, m_max | (n_max << 8) | (k_max << 16), host_param_stack, dev_param_stack,
+      (const double*)dev_a_data, (const double*)dev_b_data, (double*)dev_c_data);
+  }
+  return xs_process_format(dev_param_stack, stack_size, 0, 1.0, datatype, dev_a_data, dev_b_data, dev_c_data, m_max, n_max,
+    k_max, max_kernel_dim, def_mnk, stack_stream);
+}
+
+/* The DBM side (opencl_libsmm_acc_process with param_format != 0, smm_kernel.c:82-88 and
+   multiply.cl:96-99): ntasks 6-int records (m, n, k, a, b, c) with 0-based offsets, all of the
+   shape packed into param_format (m | n << 8 | k << 16), C += alpha * A * B. Mixed shapes
+   (param_format 0) are not handled here (-1). The signature is libxstream_b200_dbm_launch_fn_t, so
+   this function can itself be installed as the hook. */
+int libxstream_b200_dbm_launch(void* stream, double alpha, int ntasks, int param_format, const int* params_host,
+  const int* params, const double* pack_a_data, const double* pack_b_data, double* shard_c_data) {
+  const int m = param_format & 255, n = (param_format >> 8) & 255, k = (param_format >> 16) & 255;
+  (void)params_host;
+  if (0 >= ntasks) return EXIT_SUCCESS;
+  if (0 == m || 0 == n || 0 == k) return -1;
+  return xs_process_format(params, ntasks, 1, alpha, dbcsr_type_real_8, pack_a_data, pack_b_data, shard_c_data, m, n, k, 80, 1,
+    stream);
+}
+
+static int xs_process_format(const int* dev_param_stack, int stack_size, int format, double alpha, libsmm_acc_data_t datatype,
+  const void* dev_a_data, const void* dev_b_data, void* dev_c_data, int m_max, int n_max, int k_max, int max_kernel_dim,
+  c_dbcsr_acc_bool_t def_mnk, void* stack_stream) {
   xs_smm_params_t prm;
   void* stream = (NULL != stack_stream) ? stack_stream : xs_default_stream();
   void* scratch = NULL;
   size_t nbytes;
   int result;
-  (void)host_param_stack;
-  (void)c_stream;
   if (0 == stack_size) return EXIT_SUCCESS;
   if (!libxstream_b200_process_suitable(def_mnk, datatype, stack_size, m_max, n_max, k_max, max_kernel_dim)) {
     if (2 <= xs_verbosity()) {
@@ -96,6 +155,7 @@ int libsmm_acc_process(const int* host_param_stack, const int* dev_param_stack, 
   if (NULL == dev_param_stack || NULL == dev_a_data || NULL == dev_b_data || NULL == dev_c_data) return EXIT_FAILURE;
   result = xs_lazy_init();
   if (EXIT_SUCCESS != result) return result;
+  xs_autotune_if_needed(m_max, n_max, k_max, stack_size, stream);
   xs_params_lookup((int)datatype, m_max, n_max, k_max, stack_size, &prm);
   if (3 <= xs_verbosity()) {
     fprintf(stderr, "INFO LIBSMM/B200: SMM-kernel %ix%ix%i L=%i MT=%i NT=%i KP=%i WPB=%i ss=%i\n", m_max, n_max, k_max,
@@ -104,7 +164,7 @@ int libsmm_acc_process(const int* host_param_stack, const int* dev_param_stack, 
   nbytes = xs_smm_f64_scratch_bytes(stack_size, m_max, n_max, k_max, &prm);
   result = xs_scratch_alloc(&scratch, nbytes, stream);
   if (EXIT_SUCCESS == result) {
-    result = xs_record_error(xs_launch_smm_f64(dev_param_stack, stack_size, (const double*)dev_a_data,
+    result = xs_record_error(xs_launch_smm_f64_ex(dev_param_stack, stack_size, format, alpha, (const double*)dev_a_data,
                                (const double*)dev_b_data, (double*)dev_c_data, m_max, n_max, k_max, &prm, scratch, nbytes,
                                stream),
       "libsmm_acc_process");

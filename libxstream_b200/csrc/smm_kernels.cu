@@ -66,7 +66,7 @@ struct Tile {
 /* Write-back of a finished C sub-tile: each element has exactly one writer (red.global.add.f64). */
 template <int MT, int NT>
 __device__ __forceinline__ void commit_tile(double* __restrict__ C, size_t coff, const double (&acc)[MT][NT][2], int m,
-  int n, int g, int t, const Tile<MT, NT>& tl) {
+  int n, int g, int t, const Tile<MT, NT>& tl, double alpha) {
 #pragma unroll
   for (int i = 0; i < MT; ++i) {
     const int r = tl.r0 + 8 * i + g;
@@ -74,8 +74,8 @@ __device__ __forceinline__ void commit_tile(double* __restrict__ C, size_t coff,
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
         const int cc = tl.c0 + 8 * j + 2 * t;
-        if (cc < n) atomicAdd(C + coff + (size_t)cc * m + r, acc[i][j][0]);
-        if (cc + 1 < n) atomicAdd(C + coff + (size_t)(cc + 1) * m + r, acc[i][j][1]);
+        if (cc < n) atomicAdd(C + coff + (size_t)cc * m + r, alpha * acc[i][j][0]);
+        if (cc + 1 < n) atomicAdd(C + coff + (size_t)(cc + 1) * m + r, alpha * acc[i][j][1]);
       }
     }
   }
@@ -111,6 +111,7 @@ struct StackTask {
   int item_begin; /* first work item of this stack (batch) */
   int cls;        /* tile class (MT - 1) * 4 + (NT - 1) (batch) */
   int sid;        /* stack index within the call: tag of its segment-list entries */
+  double alpha;   /* C += alpha * A * B (1 for the LIBSMM ABI) */
 };
 
 /* Segment-list entry: stack index (high 8 bits) and CTA group (low 24 bits). */
@@ -220,7 +221,7 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
           const bool crossl = headcross && (segstart == p0);
           const bool crossr = tailcross && (e + 1 == p1);
           if (!crossl && !crossr) {
-            commit_tile<MT, NT>(C, (size_t)key_cur - 1, acc, m, n, g, t, tl);
+            commit_tile<MT, NT>(C, (size_t)key_cur - 1, acc, m, n, g, t, tl, tk.alpha);
           }
           else { /* piece: head slot if it continues a segment from the previous chunk, else tail */
             const int slot = crossl ? 0 : 1;
@@ -310,7 +311,7 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
           tile[i][j][0] = sum[(i * NT + j) * 2 + 0];
           tile[i][j][1] = sum[(i * NT + j) * 2 + 1];
         }
-      commit_tile<MT, NT>(C, (size_t)key - 1, tile, m, n, g, t, tl);
+      commit_tile<MT, NT>(C, (size_t)key - 1, tile, m, n, g, t, tl, tk.alpha);
     }
   }
   __syncthreads();
@@ -465,7 +466,7 @@ __device__ __forceinline__ void combine_one(const StackTask& tk, int W, int j0, 
         tile[i][j][0] = acc[(i * NT + j) * 2 + 0];
         tile[i][j][1] = acc[(i * NT + j) * 2 + 1];
       }
-    commit_tile<MT, NT>(tk.c, (size_t)xkey - 1, tile, tk.m, tk.n, g, t, tl);
+    commit_tile<MT, NT>(tk.c, (size_t)xkey - 1, tile, tk.m, tk.n, g, t, tl, tk.alpha);
   }
   __syncthreads();
 }
@@ -942,14 +943,19 @@ size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_sm
 
 int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double* b, double* c, int m, int n, int k,
   const xs_smm_params_t* prm, void* scratch, size_t scratch_bytes, void* stream) {
+  return xs_launch_smm_f64_ex(dev_stack, S, 0, 1.0, a, b, c, m, n, k, prm, scratch, scratch_bytes, stream);
+}
+
+int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, const double* a, const double* b, double* c,
+  int m, int n, int k, const xs_smm_params_t* prm, void* scratch, size_t scratch_bytes, void* stream) {
   SmmPlan pl;
   cudaStream_t s = (cudaStream_t)stream;
   if (0 >= S) return 0;
   const int smax = xs_stack_group_max();
   if (S > smax) { /* C += A*B is additive over the stack: run it in consecutive parts */
     for (int off = 0; off < S; off += smax) {
-      const int r = xs_launch_smm_f64(dev_stack + 3 * (size_t)off, min(smax, S - off), a, b, c, m, n, k, prm, scratch,
-        scratch_bytes, stream);
+      const int r = xs_launch_smm_f64_ex(dev_stack + (0 != format ? 6 : 3) * (size_t)off, min(smax, S - off), format, alpha, a, b,
+        c, m, n, k, prm, scratch, scratch_bytes, stream);
       if (0 != r) return r;
     }
     return 0;
@@ -965,11 +971,12 @@ int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double
   int* const seglist = (int*)(base + pl.off_seglist);
   void* const sort_scratch = base + pl.off_sort;
   void* prof = xs_profile_begin(s);
-  const int r = xs_stack_group(dev_stack, S, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, seglist,
+  const int r = xs_stack_group_ex(dev_stack, S, format, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, seglist,
     sort_scratch, s);
   if (0 != r) return r;
   xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
   StackTask tk = {};
+  tk.alpha = alpha;
   tk.a = a;
   tk.b = b;
   tk.c = c;
@@ -1034,6 +1041,7 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     const BatchPart& p = bp.part[q];
     sb.gidx[sb.nstacks] = q;
     sb.stack[sb.nstacks] = st[p.stack].dev_param_stack + 3 * (size_t)p.first;
+    sb.format[sb.nstacks] = 0;
     sb.S[sb.nstacks] = p.S;
     sb.off[sb.nstacks] = (int)bp.off_part[q];
     ++sb.nstacks;
@@ -1052,6 +1060,7 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     const BatchPart& p = bp.part[q];
     const libxstream_b200_stack_t& d = st[p.stack];
     StackTask tk = {};
+    tk.alpha = 1.0;
     tk.a = (const double*)d.a;
     tk.b = (const double*)d.b;
     tk.c = (double*)d.c;

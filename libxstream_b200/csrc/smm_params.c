@@ -83,7 +83,21 @@ void xs_params_default(int m, int n, int k, int stack_size, xs_smm_params_t* out
   xs_sanitize(out);
 }
 
+static float xs_mlp_minconf(void) {
+  static float v = -1.f;
+  if (0 > v) {
+    const char* const env = getenv("LIBXSTREAM_B200_MLP_MINCONF");
+    v = (NULL != env) ? (float)atof(env) : 0.5f;
+    if (0 > v) v = 0.f;
+  }
+  return v;
+}
+
 void xs_params_lookup(int type, int m, int n, int k, int stack_size, xs_smm_params_t* out) {
+  xs_params_lookup_ex(type, m, n, k, stack_size, out, NULL);
+}
+
+void xs_params_lookup_ex(int type, int m, int n, int k, int stack_size, xs_smm_params_t* out, int* source) {
   unsigned h = xs_hash(type, m, n, k) & (XS_PARAMS_CAP - 1);
   int probe, found = 0;
   pthread_rwlock_rdlock(&xs_table_lock);
@@ -97,7 +111,24 @@ void xs_params_lookup(int type, int m, int n, int k, int stack_size, xs_smm_para
     }
   }
   pthread_rwlock_unlock(&xs_table_lock);
-  if (!found) xs_params_default(m, n, k, stack_size, out);
+  if (NULL != source) *source = found ? XS_PARAMS_TUNED : XS_PARAMS_DEFAULT;
+  if (!found) {
+    int mt, nt, kp;
+    float conf = 0.f;
+    xs_params_default(m, n, k, stack_size, out);
+    if (xs_mlp_lookup(m, n, k, stack_size, &mt, &nt, &kp, &conf)) {
+      /* the prediction beats the default heuristic even when unconfident; the confidence only decides
+         whether the exhaustive tuner should check it (LIBXSTREAM_B200_AUTOTUNE) */
+      out->mt = mt;
+      out->nt = nt;
+      out->kp = kp;
+      out->chunk = 0;
+      out->wpb = 4;
+      out->generic = 0;
+      xs_sanitize(out);
+      if (NULL != source) *source = (conf >= xs_mlp_minconf()) ? XS_PARAMS_PREDICTED : XS_PARAMS_LOWCONF;
+    }
+  }
 }
 
 int xs_params_set(int type, int m, int n, int k, const xs_smm_params_t* p, double gflops) {

@@ -18,6 +18,7 @@
 #include "internal.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 /* Library-wide device error word: bit 0 = a grid barrier of the grouping sort timed out, bit 2 = a
    pipeline wait of the Ozaki GEMM timed out. */
@@ -157,6 +158,9 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
   int si = 0;
   while (si + 1 < desc.nstacks && desc.tile_begin[si + 1] <= tile) ++si;
   const int* const stack = desc.stack[si];
+  /* parameter format: 1-based (a, b, c) triples, or 6-int records with 0-based (a, b, c) at +3 */
+  const int pstride = (0 != desc.format[si]) ? 6 : 3, pbase = (0 != desc.format[si]) ? 3 : 0;
+  const int pone = (0 != desc.format[si]) ? 1 : 0;
   const int S = desc.S[si], off = desc.off[si], tb = desc.tile_begin[si], G = desc.ntiles[si];
   const int lt = tile - tb, T = kSortThreads * E;
   const int t0 = min(S, lt * T), t1 = min(S, t0 + T);
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
 
   /* phase 0: load + bucket statistics of this stack */
   {
-    const unsigned c0 = (unsigned)stack[2];
+    const unsigned c0 = (unsigned)(stack[pbase + 2] + pone);
     unsigned lo = 0xFFFFFFFFu, hi = 0u, gg = 0u;
 #pragma unroll
     for (int r = 0; r < E; ++r) {
@@ -182,8 +186,9 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
       key[r] = 0u;
       val[r] = 0ull;
       if (i < w1) {
-        const int a = stack[3 * i + 0], b = stack[3 * i + 1];
-        key[r] = (unsigned)stack[3 * i + 2];
+        const int* const e = stack + (size_t)pstride * i + pbase;
+        const int a = e[0] + pone, b = e[1] + pone;
+        key[r] = (unsigned)(e[2] + pone);
         val[r] = (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32);
       }
     }
@@ -515,9 +520,16 @@ int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned lon
 
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
+  return xs_stack_group_ex(dev_stack, S, 0, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, stream);
+}
+
+int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned* k0, unsigned long long* v0, unsigned* k1,
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
   xs_sort_batch_t d;
+  memset(&d, 0, sizeof(d));
   d.nstacks = 1;
   d.stack[0] = dev_stack;
+  d.format[0] = format;
   d.S[0] = S;
   d.off[0] = 0;
   d.gidx[0] = 0;
@@ -563,6 +575,7 @@ int libxstream_b200_device_error(int reset) {
 int xs_stack_group_profile(const int* dev_stack, int S, unsigned long long* host_stamps, int capacity, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   xs_sort_batch_t d;
+  memset(&d, 0, sizeof(d));
   d.nstacks = 1;
   d.stack[0] = dev_stack;
   d.S[0] = S;
