@@ -863,20 +863,78 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
 
 /* ------------------------------------------------------------------------------ transpose */
 
-/* One CTA per block: stage the m x n column-major block in shared memory, write it back as n x m
-   column-major (transpose.cl:28-83 semantics; a bit copy, so exact for any element type). */
+/* In-place transposes of listed blocks (transpose.cl:28-83 semantics; a bit copy, exact for any
+   element type). One CTA handles `nb` blocks at a time: all their elements are gathered into shared
+   memory with consecutive threads on consecutive elements of a block (coalesced), each block's
+   columns `ld` = m|1 elements apart (an odd stride: the transposed reads of a warp then hit distinct
+   banks), then written back as n x m column-major, again with consecutive threads on consecutive
+   output elements. */
 template <typename T>
-__global__ void xs_transpose_kernel(const int* __restrict__ trs, int offset, int S, T* __restrict__ data, int m, int n) {
+__global__ void __launch_bounds__(256) xs_transpose_kernel(const int* __restrict__ trs, int offset, int S, T* __restrict__ data,
+  int m, int n, int nb) {
   extern __shared__ unsigned char smem_raw[];
+  __shared__ int s_off[256];
   T* const buf = reinterpret_cast<T*>(smem_raw);
-  const int mn = m * n;
-  for (int blk = blockIdx.x; blk < S; blk += gridDim.x) {
-    T* const mat = data + trs[offset + blk];
-    for (int e = threadIdx.x; e < mn; e += blockDim.x) buf[e] = mat[e];
+  const int mn = m * n, ld = m | 1, bsz = ld * n, step = blockDim.x;
+  /* the thread stride as (blocks, columns, rows) for the input walk and (blocks, rows, columns) for
+     the output walk, so that indices advance by additions and carries only */
+  const int sb = step / mn, sr = step - sb * mn;
+  const int sj_in = sr / m, si_in = sr - sj_in * m;  /* input: e = b*mn + j*m + i */
+  const int si_out = sr / n, sj_out = sr - si_out * n; /* output: e = b*mn + i*n + j */
+  const int t = threadIdx.x;
+  const int tb = t / mn, tr = t - tb * mn;
+  const int tj_in = tr / m, ti_in = tr - tj_in * m, ti_out = tr / n, tj_out = tr - ti_out * n;
+  for (int b0 = blockIdx.x * nb; b0 < S; b0 += gridDim.x * nb) {
+    const int nbl = min(nb, S - b0);
+    for (int q = t; q < nbl; q += step) s_off[q] = trs[offset + b0 + q];
     __syncthreads();
-    for (int o = threadIdx.x; o < mn; o += blockDim.x) {
-      const int i = o / n, j = o - i * n; /* output (j, i) of the n x m result = input (i, j) */
-      mat[o] = buf[j * m + i];
+    { /* gather: eight independent loads in flight per thread, then the shared-memory stores */
+      int b = tb, j = tj_in, i = ti_in;
+      while (b < nbl) {
+        T v[8];
+        int pos[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          pos[u] = -1;
+          if (b < nbl) {
+            v[u] = data[s_off[b] + j * m + i];
+            pos[u] = b * bsz + j * ld + i;
+          }
+          i += si_in;
+          if (i >= m) {
+            i -= m;
+            ++j;
+          }
+          j += sj_in;
+          if (j >= n) {
+            j -= n;
+            ++b;
+          }
+          b += sb;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (pos[u] >= 0) buf[pos[u]] = v[u];
+        }
+      }
+    }
+    __syncthreads();
+    {
+      int b = tb, i = ti_out, j = tj_out;
+      while (b < nbl) { /* output (j, i) of the n x m result at i*n + j = input (i, j) */
+        data[s_off[b] + i * n + j] = buf[b * bsz + j * ld + i];
+        j += sj_out;
+        if (j >= n) {
+          j -= n;
+          ++i;
+        }
+        i += si_out;
+        if (i >= m) {
+          i -= m;
+          ++b;
+        }
+        b += sb;
+      }
     }
     __syncthreads();
   }
@@ -1122,10 +1180,19 @@ int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize
   cudaStream_t s = (cudaStream_t)stream;
   if (0 >= S) return 0;
   const int mn = m * n;
-  const size_t smem = (size_t)mn * esize;
-  int threads = ((mn + 31) / 32) * 32;
-  if (threads > 256) threads = 256;
-  const int grid = S < 64 * xs_sm_count() ? S : 64 * xs_sm_count();
+  const size_t bbytes = (size_t)(m | 1) * n * esize;
+  /* blocks per CTA: up to 24 KB of shared memory, but at least one CTA per SM when there are blocks
+     enough (small blocks would otherwise give too few CTAs) */
+  int nb = (int)((24 * 1024) / bbytes);
+  if (nb < 1) nb = 1;
+  const int per_sm = (S + xs_sm_count() - 1) / xs_sm_count();
+  if (nb > per_sm) nb = per_sm;
+  if (nb > 256) nb = 256; /* block offsets staged per CTA */
+  const size_t smem = bbytes * nb;
+  if (smem > 227 * 1024) return (int)cudaErrorInvalidValue; /* a block larger than shared memory */
+  const int threads = (nb * mn >= 256) ? 256 : ((nb * mn + 31) / 32) * 32;
+  int grid = (S + nb - 1) / nb;
+  if (grid > 16 * xs_sm_count()) grid = 16 * xs_sm_count();
   cudaError_t r;
   void* const prof = xs_profile_begin(s);
   if (8 == esize) {
@@ -1133,14 +1200,14 @@ int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize
       r = cudaFuncSetAttribute(xs_transpose_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (cudaSuccess != r) return (int)r;
     }
-    xs_transpose_kernel<unsigned long long><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned long long*)data, m, n);
+    xs_transpose_kernel<unsigned long long><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned long long*)data, m, n, nb);
   }
   else if (4 == esize) {
     if (smem > 48 * 1024) {
       r = cudaFuncSetAttribute(xs_transpose_kernel<unsigned>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (cudaSuccess != r) return (int)r;
     }
-    xs_transpose_kernel<unsigned><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned*)data, m, n);
+    xs_transpose_kernel<unsigned><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned*)data, m, n, nb);
   }
   else return (int)cudaErrorInvalidValue;
   r = cudaGetLastError();
