@@ -110,6 +110,32 @@ SIGNATURES = {
     "libxstream_b200_set_dbm_launch_fn": (None, [ctypes.c_void_p]),
     "libxstream_b200_dbm_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    # CP2K offload API (include/offload_cp2k.h)
+    "offloadGetErrorName": (ctypes.c_char_p, [ctypes.c_int]),
+    "offloadGetLastError": (ctypes.c_int, []),
+    "offloadMemsetAsync": (None, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p]),
+    "offloadMemset": (None, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t]),
+    "offloadMemcpyAsyncHtoD": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    "offloadMemcpyAsyncDtoH": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    "offloadMemcpyAsyncDtoD": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    "offloadMemcpyHtoD": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "offloadMemcpyDtoH": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "offloadMemcpyToSymbol": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "offloadEventCreate": (None, [ctypes.c_void_p]),
+    "offloadEventDestroy": (None, [ctypes.c_void_p]),
+    "offloadEventSynchronize": (None, [ctypes.c_void_p]),
+    "offloadEventRecord": (None, [ctypes.c_void_p, ctypes.c_void_p]),
+    "offloadEventQuery": (ctypes.c_bool, [ctypes.c_void_p]),
+    "offloadStreamCreate": (None, [ctypes.c_void_p]),
+    "offloadStreamDestroy": (None, [ctypes.c_void_p]),
+    "offloadStreamSynchronize": (None, [ctypes.c_void_p]),
+    "offloadStreamWaitEvent": (None, [ctypes.c_void_p, ctypes.c_void_p]),
+    "offloadMallocHost": (None, [ctypes.c_void_p, ctypes.c_size_t]),
+    "offloadMalloc": (None, [ctypes.c_void_p, ctypes.c_size_t]),
+    "offloadFree": (None, [ctypes.c_void_p]),
+    "offloadFreeHost": (None, [ctypes.c_void_p]),
+    "offloadDeviceSynchronize": (None, []),
+    "offloadEnsureMallocHeapSize": (None, [ctypes.c_size_t]),
     "libxstream_b200_process_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -55,6 +55,12 @@ int xs_record_error(int cuda_error, const char* where) {
 
 int xs_last_error(void) { return xs_error; }
 
+int xs_consume_error(void) {
+  const int e = xs_error;
+  xs_error = 0;
+  return e;
+}
+
 void xs_inject_alloc_failure(int nth) { xs_alloc_fail_countdown = nth; }
 
 static int xs_count_devices(void) {

@@ -24,6 +24,8 @@ int xs_sm_count(void);
 int xs_record_error(int cuda_error, const char* where);
 /** Last recorded error code (0 if none). */
 int xs_last_error(void);
+/** Last recorded error code, and reset the slot. */
+int xs_consume_error(void);
 /** LIBSMM initialised (lazily, reference counted once) and the active device current. */
 int xs_smm_ensure_init(void);
 /** Verbosity from LIBXSTREAM_B200_VERBOSE (0 = quiet). */
