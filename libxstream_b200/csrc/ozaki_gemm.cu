@@ -280,17 +280,24 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * kBN + c0), v);
         tmem_ld_wait();
-        if (rok) {
+        if (rok) { /* all 32 loads of the chunk first, then the updates and the stores (no load waits for a
+                      store it cannot be proven independent of) */
+          double* const crow = args.C + row + (long long)(n0 + c0) * args.ldc;
+          const int ncol = min(32, args.N - (n0 + c0));
+          const bool read_c = !beta_now || 0.0 != args.beta;
+          double cv[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) cv[j] = (j < ncol && read_c) ? crow[(long long)j * args.ldc] : 0.0;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
-            const int col = n0 + c0 + j;
-            if (col < args.N) {
-              double* const p = args.C + row + (long long)col * args.ldc;
-              double c = beta_now ? ((0.0 == args.beta) ? 0.0 : args.beta * *p) : *p;
-              const int iv = (int)v[j];
-              if (0 != iv) c = add_scaled(c, iv, ear + s_eb[c0 + j] + eshift, args.alpha);
-              *p = c;
-            }
+            double c = beta_now ? args.beta * cv[j] : cv[j];
+            const int iv = (int)v[j];
+            if (0 != iv) c = add_scaled(c, iv, ear + s_eb[c0 + j] + eshift, args.alpha);
+            cv[j] = c;
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            if (j < ncol) crow[(long long)j * args.ldc] = cv[j];
           }
         }
       }
