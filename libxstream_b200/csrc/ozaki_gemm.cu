@@ -50,6 +50,7 @@ constexpr int kMaxGroups = 2 * kMaxSlices - 1;
 constexpr int kKChunkBlocks = 16384 / kBK; /* k-blocks per launch: keeps every diagonal's int32 sum exact */
 constexpr int kATileBytes = kBM * kBK, kBTileBytes = kBN * kBK;
 constexpr int kGemmThreads = 192;
+constexpr int kGroupM = 8; /* row panels per rasterization group */
 constexpr unsigned kErrOzakiTimeout = 4u; /* device error word bit: an Ozaki pipeline wait timed out */
 
 /* ------------------------------------------------------------------------------ slicing */
@@ -192,7 +193,16 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   unsigned* const abort = args.abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * kBN, m0 = blockIdx.y * kBM;
+  /* tile order: groups of kGroupM row panels sweep the column panels together, so that the CTAs of
+     one wave share their A row panels and B column panels in L2 */
+  int n0, m0;
+  {
+    const int ntm = (args.M + kBM - 1) / kBM, ntn = (args.N + kBN - 1) / kBN;
+    const int id = blockIdx.x, per_group = kGroupM * ntn, g = id / per_group, first = g * kGroupM;
+    const int gsize = min(kGroupM, ntm - first), r = id - g * per_group;
+    m0 = (first + r % gsize) * kBM;
+    n0 = (r / gsize) * kBN;
+  }
   if (0 == threadIdx.x) {
     for (int i = 0; i < kStages; ++i) {
       mbar_init(&full[i], 1);
@@ -452,7 +462,7 @@ int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, c
     smem_set = 1;
   }
   const int nkb = (K + kBK - 1) / kBK;
-  const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
+  const dim3 grid(((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM));
   for (int kb0 = 0; kb0 < nkb; kb0 += kKChunkBlocks) {
     args.kb0 = kb0;
     args.kb1 = (kb0 + kKChunkBlocks < nkb) ? kb0 + kKChunkBlocks : nkb;
