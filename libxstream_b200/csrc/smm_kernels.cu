@@ -24,6 +24,7 @@
  *   The result is bitwise reproducible from run to run, unlike FP atomics.
  */
 #include "internal.h"
+#include "tc_ptx.cuh"
 #include "../../include/libxstream_b200.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -117,6 +118,65 @@ struct StackTask {
 /* Segment-list entry: stack index (high 8 bits) and CTA group (low 24 bits). */
 __device__ __forceinline__ int seg_tag(int sid, int group) { return (sid << 24) | group; }
 
+/* CTA-level merge of the warps' partial tiles. Chains start at warp 0's head piece (a segment
+   entering the CTA) and at every tail piece (a segment starting in that warp's chunk); a chain
+   continues through the head pieces of the following warps while the previous piece reaches the end
+   of its chunk. A chain that stays inside the CTA is written back at once; one that crosses the CTA's
+   boundaries becomes a CTA-level piece in global scratch for the combine kernel. piece_at(w, slot)
+   is warp w's head (slot 0) or tail (slot 1) piece in shared memory, [REGS][32] doubles; meta[w][4]
+   holds its head / head-spans / tail flags. Called by all threads after a CTA barrier. */
+template <int MT, int NT, typename PieceAt>
+__device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int sub, int* __restrict__ seglist,
+  const int* meta, int W, PieceAt piece_at) {
+  constexpr int REGS = MT * NT * 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub = tk.nsub;
+  for (int start = 0; start < 2; ++start) {
+    const bool from_head = (0 == start);
+    if (from_head && 0 != warp) continue;
+    if (0 == meta[warp * 4 + (from_head ? 0 : 2)]) continue;
+    double sum[REGS];
+    const double* src = piece_at(warp, from_head ? 0 : 1) + lane;
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) sum[r] = src[r * 32];
+    bool spans = from_head ? (0 != meta[warp * 4 + 1]) : true;
+    int cur = warp;
+    while (spans && cur + 1 < W && group * W + cur + 1 < nchunks) {
+      ++cur;
+      src = piece_at(cur, 0) + lane;
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) sum[r] += src[r * 32];
+      spans = (0 != meta[cur * 4 + 1]);
+    }
+    const int c_first = group * W + warp; /* chunk where this chain starts */
+    if (from_head || spans) { /* the segment crosses a CTA boundary: CTA-level piece */
+      const int slot = from_head ? 2 * group : 2 * group + 1;
+      double* const dst = tk.pieces + ((size_t)slot * nsub + sub) * REGS * 32 + lane;
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) dst[r * 32] = sum[r];
+      if (!from_head && 0 == sub && 0 == lane) {
+        const int slotidx = atomicAdd(seglist, 1);
+        seglist[1 + slotidx] = seg_tag(tk.sid, group);
+      }
+    }
+    else {
+      const int p1 = min((c_first + 1) * L, S);
+      const unsigned key = tk.keys[p1 - 1]; /* a tail piece belongs to the last segment of its chunk */
+      double tile[MT][NT][2];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          tile[i][j][0] = sum[(i * NT + j) * 2 + 0];
+          tile[i][j][1] = sum[(i * NT + j) * 2 + 1];
+        }
+      Tile<MT, NT> tl;
+      tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
+      commit_tile<MT, NT>(tk.c, (size_t)key - 1, tile, tk.m, tk.n, g, t, tl, tk.alpha);
+    }
+  }
+}
+
 /* One work item of the stack kernel: CTA group `group` (W = blockDim.x / 32 consecutive chunks of
    L grouped entries) and warp sub-tile `sub` of C (8*MT x 8*NT) of one stack. M_, N_, K_ > 0 make
    the block shape a compile-time constant (every fragment load is then one load at an immediate
@@ -137,8 +197,7 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
   double* __restrict__ const C = tk.c;
   const unsigned* __restrict__ const keys = tk.keys;
   const unsigned long long* __restrict__ const vals = tk.vals;
-  const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub_n = tk.nsub_n, nsub = tk.nsub;
-  double* __restrict__ const pieces = tk.pieces;
+  const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub_n = tk.nsub_n;
   const int W = blockDim.x >> 5;
   double* const sp = smem;                                       /* [W][2][REGS][32] */
   int* const meta = (int*)(smem + (size_t)W * 2 * REGS * 32);    /* [W][4]: head, head_spans, tail, spare */
@@ -269,51 +328,8 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
     }
   }
   __syncthreads();
-  /* CTA-level merge. Chains start at warp 0's head piece (a segment entering the CTA) and at every
-     tail piece (a segment starting in that warp's chunk); a chain continues through the head pieces
-     of the following warps while the previous piece reaches the end of its chunk. */
-  for (int start = 0; start < 2; ++start) {
-    const bool from_head = (0 == start);
-    if (from_head && 0 != warp) continue;
-    if (0 == meta[warp * 4 + (from_head ? 0 : 2)]) continue;
-    double sum[REGS];
-    const double* src = sp + ((size_t)(warp * 2 + (from_head ? 0 : 1)) * REGS) * 32 + lane;
-#pragma unroll
-    for (int r = 0; r < REGS; ++r) sum[r] = src[r * 32];
-    bool spans = from_head ? (0 != meta[warp * 4 + 1]) : true;
-    int cur = warp;
-    while (spans && cur + 1 < W && group * W + cur + 1 < nchunks) {
-      ++cur;
-      src = sp + ((size_t)(cur * 2) * REGS) * 32 + lane;
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) sum[r] += src[r * 32];
-      spans = (0 != meta[cur * 4 + 1]);
-    }
-    const int c_first = group * W + warp; /* chunk where this chain starts */
-    if (from_head || spans) { /* the segment crosses a CTA boundary: CTA-level piece */
-      const int slot = from_head ? 2 * group : 2 * group + 1;
-      double* const dst = pieces + ((size_t)slot * nsub + sub) * REGS * 32 + lane;
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) dst[r * 32] = sum[r];
-      if (!from_head && 0 == sub && 0 == lane) {
-        const int slotidx = atomicAdd(seglist, 1);
-        seglist[1 + slotidx] = seg_tag(tk.sid, group);
-      }
-    }
-    else {
-      const int p1 = min((c_first + 1) * L, S);
-      const unsigned key = keys[p1 - 1]; /* a tail piece belongs to the last segment of its chunk */
-      double tile[MT][NT][2];
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-          tile[i][j][0] = sum[(i * NT + j) * 2 + 0];
-          tile[i][j][1] = sum[(i * NT + j) * 2 + 1];
-        }
-      commit_tile<MT, NT>(C, (size_t)key - 1, tile, m, n, g, t, tl, tk.alpha);
-    }
-  }
+  cta_merge<MT, NT>(tk, group, sub, seglist, meta, W,
+    [&](int w, int slot) -> const double* { return sp + ((size_t)(w * 2 + slot) * REGS) * 32; });
   __syncthreads();
 }
 
@@ -324,6 +340,255 @@ __global__ void __launch_bounds__(128, smm_min_blocks(MT, NT))
   if (0 != *(volatile const unsigned*)err) return; /* the grouping failed: write nothing */
   const int group = blockIdx.x / tk.nsub, sub = blockIdx.x - group * tk.nsub;
   smm_item<M_, N_, K_, MT, NT, KP>(tk, group, sub, seglist, smem);
+}
+
+/* ------------------------------------------------- staged stack kernel (bulk copies into shared memory) */
+
+/* Device error word bit: a wait of the staged stack kernel for its bulk copies timed out. */
+constexpr unsigned kErrStagedTimeout = 16u;
+
+/* Geometry of the staged kernel for an M_ x N_ x K_ block shape whose whole C block is one warp tile
+   (MT = ceil(M_/8), NT = ceil(N_/8), both <= 4). A stage holds the 16-byte-aligned windows around one
+   A block and one B block as the bulk copies bring them (a block that starts 8 bytes past a 16-byte
+   boundary is copied from that boundary, so a window is at most 8 bytes longer than its block). Per
+   warp: a ring of R stages, reused for the warp's two partial tiles once the ring is drained; then R
+   mbarriers per warp and the merge metadata [W][4]. */
+template <int M_, int N_, int K_>
+struct Staged {
+  static constexpr int MT = (M_ + 7) / 8, NT = (N_ + 7) / 8, REGS = MT * NT * 2, KS = (K_ + 3) / 4;
+  static constexpr int SA = (M_ * K_ * 8 + 8 + 15) / 16 * 16;
+  static constexpr int SB = (K_ * N_ * 8 + 8 + 15) / 16 * 16;
+  static constexpr int STAGE = SA + SB;
+  static constexpr int PIECES = 2 * REGS * 32 * (int)sizeof(double);
+  /* k-index of lane t (t = lane % 4) in DMMA step s. The four k-indices of a step may be any four
+     indices of the block as long as A and B use the same ones, so they are chosen to spread the
+     warp's shared-memory fragment reads over all banks: lanes t = 0..3 read columns kk(s, t) of A
+     (rows of B), ld = M_ (N_) doubles apart. With stride Q between them (kk = base + Q*t) the columns
+     start Q*M_*8 bytes apart; when Q*M_ mod 16 is 4 or 12 (in doubles) the four 4-lane groups of a
+     half-warp land on four disjoint sets of banks. Full groups of 4*Q indices use stride Q; the
+     remainder uses Q too when that costs no extra step, else stride 1. */
+  static constexpr bool spread(int q) { return ((q * M_) % 16 == 4 || (q * M_) % 16 == 12) && ((q * N_) % 16 == 4 || (q * N_) % 16 == 12); }
+  static constexpr int Q = spread(1) ? 1 : (spread(2) ? 2 : (spread(4) ? 4 : 1));
+  static constexpr int GQ = (K_ / (4 * Q)) * Q; /* steps in full groups */
+  static constexpr int RS = KS - GQ;             /* remainder steps */
+  static constexpr int QR = (RS == Q) ? Q : 1;
+  __device__ static __forceinline__ int kidx(int s, int t) {
+    return (s < GQ) ? 4 * Q * (s / Q) + (s % Q) + Q * t
+                    : 4 * GQ + ((1 == QR) ? 4 * (s - GQ) + t : (s - GQ) + QR * t);
+  }
+  __host__ __device__ static constexpr int warp_bytes(int R) { return (R * STAGE > PIECES) ? R * STAGE : PIECES; }
+  __host__ __device__ static constexpr size_t smem_bytes(int W, int R) {
+    return (size_t)W * warp_bytes(R) + (size_t)W * R * sizeof(uint64_t) + (size_t)W * 4 * sizeof(int);
+  }
+};
+
+/* Waits (bounded, ignoring the abort word) for a stage whose copies were issued, so that no copy
+   still lands in shared memory after the warp gave up. */
+__device__ __forceinline__ void drain_stage(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!xs_tc::mbar_try_wait(bar, parity) && clock64() - t0 < 400000000ll) {
+  }
+}
+
+/* The staged stack kernel: the same chunks, segments, pieces and CTA merge as the register kernel,
+   but lane 0 of each warp streams the A and B blocks of the next R-1 entries of its chunk into the
+   warp's shared-memory ring with bulk copies (cp.async.bulk, completion counted in bytes on one
+   mbarrier per stage), and the tensor pipe takes every DMMA fragment from shared memory. The L2
+   latency is then hidden behind whole entries instead of one k-panel, and no registers hold data in
+   flight. The entries' keys and payloads sit in registers (lane j holds entries j and 32 + j of the
+   current window) and are broadcast with shuffles. For block shapes whose C block is one warp tile.
+   Every wait is bounded: a copy that does not land in time sets the grouping error word (the
+   combine then writes nothing) and a device error bit, and the warp stops once the copies it has in
+   flight have landed (again bounded). */
+template <int M_, int N_, int K_, int R>
+__global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8))
+  xs_smm_staged_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, unsigned* __restrict__ err,
+    unsigned* __restrict__ dev_err) {
+  using G = Staged<M_, N_, K_>;
+  constexpr int MT = G::MT, NT = G::NT, REGS = G::REGS, KS = G::KS;
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  if (0 != *(volatile const unsigned*)err) return;
+  const int W = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int group = blockIdx.x;
+  unsigned char* const ring = smraw + (size_t)warp * G::warp_bytes(R);
+  uint64_t* const bar = (uint64_t*)(smraw + (size_t)W * G::warp_bytes(R)) + warp * R;
+  int* const meta = (int*)(smraw + (size_t)W * G::warp_bytes(R) + (size_t)W * R * sizeof(uint64_t));
+  if (0 == lane) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) xs_tc::mbar_init(&bar[q], 1);
+    xs_tc::fence_barrier_init();
+    meta[warp * 4 + 0] = 0;
+    meta[warp * 4 + 1] = 0;
+    meta[warp * 4 + 2] = 0;
+  }
+  __syncwarp();
+  const double* __restrict__ const A = tk.a;
+  const double* __restrict__ const B = tk.b;
+  const unsigned* __restrict__ const keys = tk.keys;
+  const unsigned long long* __restrict__ const vals = tk.vals;
+  const int S = tk.S, L = tk.L;
+  const int chunk = group * W + warp;
+  Tile<MT, NT> tl;
+  tl.init(0, 1, M_, N_, g);
+  double acc[MT][NT][2], hacc[MT][NT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = hacc[i][j][0] = hacc[i][j][1] = 0.0;
+  int head = 0, hspans = 0, tail = 0;
+  bool bad = false;
+  if (chunk < tk.nchunks) {
+    const int p0 = chunk * L, p1 = min(p0 + L, S);
+    const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
+    const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
+    int wb = p0; /* first entry of the current window */
+    unsigned kc = 0u, kn = 0u;
+    unsigned long long vc = 0ull, vn = 0ull;
+    if (p0 + lane < p1) {
+      kc = keys[p0 + lane];
+      vc = vals[p0 + lane];
+    }
+    if (p0 + 32 + lane < p1) {
+      kn = keys[p0 + 32 + lane];
+      vn = vals[p0 + 32 + lane];
+    }
+    auto key_of = [&](int e) -> unsigned { /* e - wb in [0, 64) */
+      const int i = e - wb;
+      const unsigned x0 = __shfl_sync(FULL, kc, i & 31), x1 = __shfl_sync(FULL, kn, i & 31);
+      return (i < 32) ? x0 : x1;
+    };
+    auto val_of = [&](int e) -> unsigned long long {
+      const int i = e - wb;
+      const unsigned long long x0 = __shfl_sync(FULL, vc, i & 31), x1 = __shfl_sync(FULL, vn, i & 31);
+      return (i < 32) ? x0 : x1;
+    };
+    /* lane 0: bulk copies of entry e's A and B windows into stage (e - p0) % R */
+    auto issue = [&](int e, unsigned long long v) {
+      if (0 == lane) {
+        unsigned char* const dst = ring + ((e - p0) % R) * G::STAGE;
+        const uintptr_t as = (uintptr_t)(A + ((unsigned)v - 1u)), bs = (uintptr_t)(B + ((unsigned)(v >> 32) - 1u));
+        const uintptr_t a0 = as & ~(uintptr_t)15, a1 = (as + (uintptr_t)M_ * K_ * 8 + 15) & ~(uintptr_t)15;
+        const uintptr_t b0 = bs & ~(uintptr_t)15, b1 = (bs + (uintptr_t)K_ * N_ * 8 + 15) & ~(uintptr_t)15;
+        uint64_t* const sb = &bar[(e - p0) % R];
+        xs_tc::mbar_arrive_expect_tx(sb, (uint32_t)((a1 - a0) + (b1 - b0)));
+        xs_tc::bulk_load(dst, (const void*)a0, (uint32_t)(a1 - a0), sb);
+        xs_tc::bulk_load(dst + G::SA, (const void*)b0, (uint32_t)(b1 - b0), sb);
+      }
+    };
+    for (int q = 0; q < R - 1 && p0 + q < p1; ++q) issue(p0 + q, val_of(p0 + q));
+    int issued = min(R - 1, p1 - p0), segstart = p0, e = p0;
+    unsigned key_cur = key_of(p0);
+    for (; e < p1; ++e) {
+      if (e - wb == 32) { /* next window of entry info (its loads have 32 - R entries to land) */
+        wb += 32;
+        kc = kn;
+        vc = vn;
+        kn = 0u;
+        vn = 0ull;
+        if (wb + 32 + lane < p1) {
+          kn = keys[wb + 32 + lane];
+          vn = vals[wb + 32 + lane];
+        }
+      }
+      if (e + R - 1 < p1) { /* refill the stage that entry e - 1 used */
+        issue(e + R - 1, val_of(e + R - 1));
+        ++issued;
+      }
+      const unsigned long long v = val_of(e);
+      const int st = (e - p0) % R;
+      const bool ok = __all_sync(FULL, xs_tc::mbar_wait(&bar[st], (uint32_t)(((e - p0) / R) & 1), err, 2u) ? 1 : 0);
+      if (!ok) {
+        bad = true;
+        break;
+      }
+      const double* const sA = (const double*)(ring + st * G::STAGE) + (((uintptr_t)(A + ((unsigned)v - 1u)) >> 3) & 1u);
+      const double* const sB =
+        (const double*)(ring + st * G::STAGE + G::SA) + (((uintptr_t)(B + ((unsigned)(v >> 32) - 1u)) >> 3) & 1u);
+#pragma unroll
+      for (int ks = 0; ks < KS; ++ks) {
+        const int kk = G::kidx(ks, t);
+        double fa[MT], fb[NT];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) fa[i] = (kk < K_ && tl.rok[i]) ? sA[kk * M_ + 8 * i + g] : 0.0;
+#pragma unroll
+        for (int j = 0; j < NT; ++j) fb[j] = (kk < K_ && tl.cok[j]) ? sB[kk * N_ + 8 * j + g] : 0.0;
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], fa[i], fb[j]);
+      }
+      const bool last = (e + 1 == p1);
+      const unsigned key_nxt = key_of(last ? e : e + 1);
+      if (last || key_nxt != key_cur) { /* the segment ends with entry e */
+        const bool crossl = headcross && (segstart == p0);
+        const bool crossr = tailcross && last;
+        if (!crossl && !crossr) commit_tile<MT, NT>(tk.c, (size_t)key_cur - 1, acc, M_, N_, g, t, tl, tk.alpha);
+        else if (!crossr) { /* continues a segment of the previous chunk: head piece */
+#pragma unroll
+          for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+              hacc[i][j][0] = acc[i][j][0];
+              hacc[i][j][1] = acc[i][j][1];
+            }
+          head = 1;
+        }
+        else if (crossl) { /* the whole chunk is one segment crossing both ends */
+          head = 1;
+          hspans = 1;
+        }
+        else tail = 1;
+        if (!crossr) {
+#pragma unroll
+          for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        }
+        segstart = e + 1;
+      }
+      key_cur = key_nxt;
+      __syncwarp();
+    }
+    if (bad) { /* entries e .. issued - 1 have copies in flight */
+      for (int q = e - p0; q < issued; ++q) drain_stage(&bar[q % R], (uint32_t)((q / R) & 1));
+    }
+  }
+  __syncwarp();
+  if (!bad) { /* the ring is drained: the warp's pieces go to its own region */
+    double* const sp = (double*)ring; /* [2][REGS][32] */
+    if (head) {
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          sp[((i * NT + j) * 2 + 0) * 32 + lane] = hspans ? acc[i][j][0] : hacc[i][j][0];
+          sp[((i * NT + j) * 2 + 1) * 32 + lane] = hspans ? acc[i][j][1] : hacc[i][j][1];
+        }
+    }
+    if (tail) {
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          sp[(REGS + (i * NT + j) * 2 + 0) * 32 + lane] = acc[i][j][0];
+          sp[(REGS + (i * NT + j) * 2 + 1) * 32 + lane] = acc[i][j][1];
+        }
+    }
+    if (0 == lane) {
+      meta[warp * 4 + 0] = head;
+      meta[warp * 4 + 1] = hspans;
+      meta[warp * 4 + 2] = tail;
+    }
+  }
+  if (__syncthreads_or(bad ? 1 : 0)) {
+    if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
+    return;
+  }
+  cta_merge<MT, NT>(tk, group, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
+    return (const double*)(smraw + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
+  });
 }
 
 /* Task table of a batch (kernel parameter: read through the constant bank). */
@@ -589,11 +854,29 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   return 0;
 }
 
+/* The combine kernel of one stack (CTA-crossing segments), MT x NT warp tiles. */
+template <int MT, int NT>
+cudaError_t launch_combine(const SmmPlan& pl, const StackTask& tk, const int* seglist, const unsigned* err, cudaStream_t s) {
+  static int csmem_set = 0;
+  const int cgrid = max(1, min(pl.ngroups * pl.nsub, 2 * xs_sm_count()));
+  const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (MT * NT * 2) * 32;
+  if (!csmem_set) {
+    const cudaError_t r = cudaFuncSetAttribute(xs_smm_combine_kernel<MT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+    if (cudaSuccess != r) return r;
+    csmem_set = 1;
+  }
+  void* prof = xs_profile_begin(s);
+  xs_smm_combine_kernel<MT, NT><<<cgrid, 32 * kCombineWarps, csmem, s>>>(tk, pl.W, seglist, err);
+  const cudaError_t r = cudaGetLastError();
+  xs_profile_end(prof, "combine", 0.0, 0.0, s);
+  return r;
+}
+
 template <int M_, int N_, int K_, int MT, int NT, int KP>
 cudaError_t launch_dmma(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err, cudaStream_t s,
   int* occ) {
   cudaError_t r;
-  static int smem_set = 0, csmem_set = 0; /* per template instance; setting them twice is harmless */
+  static int smem_set = 0; /* per template instance; setting it twice is harmless */
   const size_t smem = smm_smem_bytes<MT, NT>(pl.W);
   if (smem > 48 * 1024 && smem_set < (int)smem) {
     r = cudaFuncSetAttribute(xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -610,19 +893,31 @@ cudaError_t launch_dmma(const SmmPlan& pl, const StackTask& tk, int* seglist, co
   if (cudaSuccess != r) return r;
   const double m = tk.m, n = tk.n, k = tk.k;
   xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
-  if (pl.no_combine) return cudaSuccess;
-  const int cgrid = max(1, min(pl.ngroups * pl.nsub, 2 * xs_sm_count()));
-  const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (MT * NT * 2) * 32;
-  if (!csmem_set) {
-    r = cudaFuncSetAttribute(xs_smm_combine_kernel<MT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+  return pl.no_combine ? cudaSuccess : launch_combine<MT, NT>(pl, tk, seglist, err, s);
+}
+
+/* The staged kernel of one block shape with an R-deep ring per warp, then the combine. */
+template <int M_, int N_, int K_, int R>
+cudaError_t launch_staged(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err, cudaStream_t s,
+  int* occ) {
+  using G = Staged<M_, N_, K_>;
+  cudaError_t r;
+  static int smem_set = 0;
+  const size_t smem = G::smem_bytes(pl.W, R);
+  if (smem > 48 * 1024 && smem_set < (int)smem) {
+    r = cudaFuncSetAttribute(xs_smm_staged_kernel<M_, N_, K_, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (cudaSuccess != r) return r;
-    csmem_set = 1;
+    smem_set = (int)smem;
   }
-  prof = xs_profile_begin(s);
-  xs_smm_combine_kernel<MT, NT><<<cgrid, 32 * kCombineWarps, csmem, s>>>(tk, pl.W, seglist, err);
+  if (nullptr != occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_staged_kernel<M_, N_, K_, R>, 32 * pl.W, smem);
+  if (1 != pl.nsub) return cudaErrorInvalidValue; /* one warp tile per C block */
+  void* prof = xs_profile_begin(s);
+  xs_smm_staged_kernel<M_, N_, K_, R><<<pl.ngroups, 32 * pl.W, smem, s>>>(tk, seglist, (unsigned*)err, xs_device_error_ptr());
   r = cudaGetLastError();
-  xs_profile_end(prof, "combine", 0.0, 0.0, s);
-  return r;
+  if (cudaSuccess != r) return r;
+  const double m = M_, n = N_, k = K_;
+  xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
+  return pl.no_combine ? cudaSuccess : launch_combine<G::MT, G::NT>(pl, tk, seglist, err, s);
 }
 
 /* Runtime-shape kernels: any (m, n, k), warp sub-tile MT x NT, KP in {2, 4}. */
@@ -640,15 +935,25 @@ struct SpecEntry {
   launch_fn_t fn;
 };
 #define XS_SPEC(S, MT, KP) {S, S, S, MT, MT, KP, &launch_dmma<S, S, S, MT, MT, KP>}
+#define XS_STAGED(S, R) {S, S, S, (S + 7) / 8, (S + 7) / 8, 0, &launch_staged<S, S, S, R>}
 static const SpecEntry spec_table[] = {
-  XS_SPEC(4, 1, 1), XS_SPEC(5, 1, 2), XS_SPEC(8, 1, 2), XS_SPEC(9, 2, 3), XS_SPEC(13, 2, 2), XS_SPEC(13, 2, 4),
-  XS_SPEC(16, 2, 2), XS_SPEC(16, 2, 4), XS_SPEC(22, 3, 2), XS_SPEC(22, 3, 3), XS_SPEC(23, 3, 2), XS_SPEC(23, 3, 3),
-  XS_SPEC(26, 4, 2), XS_SPEC(26, 4, 4), XS_SPEC(32, 4, 2), XS_SPEC(32, 4, 4), XS_SPEC(45, 3, 2), XS_SPEC(45, 3, 4),
-  XS_SPEC(64, 4, 2), XS_SPEC(64, 4, 4),
+  XS_SPEC(4, 1, 1), XS_SPEC(5, 1, 2), XS_SPEC(8, 1, 2), XS_SPEC(9, 2, 3), XS_SPEC(16, 2, 2), XS_SPEC(16, 2, 4),
+  XS_SPEC(32, 4, 2), XS_SPEC(32, 4, 4), XS_SPEC(45, 3, 2), XS_SPEC(45, 3, 4), XS_SPEC(64, 4, 2), XS_SPEC(64, 4, 4),
+};
+
+/* Shapes with a staged kernel: it runs whenever the warp tile covers the whole C block (any kp),
+   unless the runtime-shape kernel is forced (generic). For block sizes that are multiples of 8 the
+   column stride puts every column on the same banks and staging does not pay; those keep the
+   register kernel. */
+static const SpecEntry staged_table[] = {
+  XS_STAGED(13, 2), XS_STAGED(22, 2), XS_STAGED(23, 2), XS_STAGED(26, 2),
 };
 
 launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
   if (0 == prm->generic) {
+    for (const SpecEntry& e : staged_table) {
+      if (e.m == m && e.n == n && e.k == k && e.mt == prm->mt && e.nt == prm->nt) return e.fn;
+    }
     for (const SpecEntry& e : spec_table) {
       if (e.m == m && e.n == n && e.k == k && e.mt == prm->mt && e.nt == prm->nt && e.kp == prm->kp) return e.fn;
     }
@@ -979,16 +1284,21 @@ extern "C" {
 
 int xs_smm_f64_specialized(int m, int n, int k, int* mt_kp_pairs, int capacity) {
   int count = 0;
-  for (const SpecEntry& e : spec_table) {
-    if (e.m == m && e.n == n && e.k == k) {
-      if (count < capacity && nullptr != mt_kp_pairs) {
-        mt_kp_pairs[3 * count + 0] = e.mt;
-        mt_kp_pairs[3 * count + 1] = e.nt;
-        mt_kp_pairs[3 * count + 2] = e.kp;
+  auto scan = [&](const SpecEntry* table, size_t len) {
+    for (size_t i = 0; i < len; ++i) {
+      const SpecEntry& e = table[i];
+      if (e.m == m && e.n == n && e.k == k) {
+        if (count < capacity && nullptr != mt_kp_pairs) {
+          mt_kp_pairs[3 * count + 0] = e.mt;
+          mt_kp_pairs[3 * count + 1] = e.nt;
+          mt_kp_pairs[3 * count + 2] = e.kp;
+        }
+        ++count;
       }
-      ++count;
     }
-  }
+  };
+  scan(staged_table, sizeof(staged_table) / sizeof(*staged_table)); /* staged kernels first (kp = 0) */
+  scan(spec_table, sizeof(spec_table) / sizeof(*spec_table));
   return count;
 }
 
