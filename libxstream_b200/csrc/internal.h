@@ -142,6 +142,8 @@ typedef struct xs_sort_batch_t {
   int off[XS_MAX_BATCH];        /* first output position of each stack */
   int tile_begin[XS_MAX_BATCH]; /* filled by the launcher */
   int ntiles[XS_MAX_BATCH];     /* filled by the launcher */
+  int* zero;                    /* nzero ints the grouping kernel sets to 0 before it ends (or nullptr) */
+  int nzero;
 } xs_sort_batch_t;
 size_t xs_sort_ctl_bytes(void);
 /** Zero the call's control block (barrier, error flag, queue, statistics of nstacks stacks). */
@@ -159,8 +161,10 @@ int xs_stack_group_fits(const xs_sort_batch_t* desc);
     (xs_sort_clear_ctl) before the first launch of the call. */
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
+/** As xs_stack_group, for either parameter format; also zeroes nzero ints at zero (nullptr: none). */
 int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned* k0, unsigned long long* v0, unsigned* k1,
-  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
+  void* stream);
 int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
 /** Device addresses inside the sort scratch: the work-queue counters of the stack kernels (one per

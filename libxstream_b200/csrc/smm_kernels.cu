@@ -35,6 +35,28 @@ namespace {
 /* Warps of the combine kernel (its warp partials go through dynamic shared memory). */
 constexpr int kCombineWarps = 16;
 
+/* Programmatic dependent launch: a kernel launched with pdl_launch may be scheduled while the
+   kernel before it in the stream is still running (once that kernel's CTAs have all passed
+   pdl_trigger or exited); it must call pdl_wait before it reads anything its predecessor writes.
+   Both are no-ops for a kernel launched the ordinary way. */
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 /* Bring a block of `count` contiguous doubles into L2 (one prefetch per 128-byte line, by 32 lanes). */
 __device__ __forceinline__ void prefetch_block_l2(const double* p, int count, int lane) {
   for (int x = 16 * lane; x < count + 15; x += 16 * 32) {
@@ -113,24 +135,67 @@ struct StackTask {
   int cls;        /* tile class (MT - 1) * 4 + (NT - 1) (batch) */
   int sid;        /* stack index within the call: tag of its segment-list entries */
   double alpha;   /* C += alpha * A * B (1 for the LIBSMM ABI) */
+  int* arrive;    /* per (CTA group, sub-tile) arrival counters of CTA-crossing segments, zero at launch:
+                     the stack kernel combines them itself; nullptr: they go to the combine kernel */
 };
 
 /* Segment-list entry: stack index (high 8 bits) and CTA group (low 24 bits). */
 __device__ __forceinline__ int seg_tag(int sid, int group) { return (sid << 24) | group; }
 
+/* Groups j0 <= j <= j1 (j0, j1 returned) that hold entries of the segment with key x, for a segment
+   that the CTA group j holds and that crosses j's first boundary (head: entry j*Lc - 1 has key x)
+   and/or its last one (tail: entry (j+1)*Lc has key x). Keys are sorted, so the boundaries a segment
+   crosses are consecutive: one warp tests 32 boundaries per round (one load per lane). */
+__device__ __forceinline__ void segment_groups(const StackTask& tk, int j, unsigned x, bool head, bool tail, int& j0,
+  int& j1) {
+  const int lane = threadIdx.x & 31, Lc = tk.L * (blockDim.x >> 5);
+  const unsigned* __restrict__ const keys = tk.keys;
+  j0 = j;
+  if (head) { /* boundary j - q (start of group j - q) is crossed iff entry (j - q) * Lc - 1 has key x */
+    for (int q0 = 1;; q0 += 32) {
+      const int gq = j - q0 - lane;
+      const bool crossed = (gq >= 1) && __ldcg(keys + (size_t)gq * Lc - 1) == x;
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, crossed);
+      if (0xFFFFFFFFu != m) {
+        j0 = j - q0 - (__ffs(~m) - 1);
+        break;
+      }
+    }
+  }
+  j1 = j;
+  if (tail) { /* group j + 1 holds x; group j + q (q >= 2) does iff its first entry has key x */
+    for (int q0 = 2;; q0 += 32) {
+      const int gq = j + q0 + lane;
+      const bool crossed = (gq < tk.ngroups) && __ldcg(keys + (size_t)gq * Lc) == x;
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, crossed);
+      if (0xFFFFFFFFu != m) {
+        j1 = j + q0 - 1 + (__ffs(~m) - 1);
+        break;
+      }
+    }
+  }
+}
+
 /* CTA-level merge of the warps' partial tiles. Chains start at warp 0's head piece (a segment
    entering the CTA) and at every tail piece (a segment starting in that warp's chunk); a chain
    continues through the head pieces of the following warps while the previous piece reaches the end
    of its chunk. A chain that stays inside the CTA is written back at once; one that crosses the CTA's
-   boundaries becomes a CTA-level piece in global scratch for the combine kernel. piece_at(w, slot)
-   is warp w's head (slot 0) or tail (slot 1) piece in shared memory, [REGS][32] doubles; meta[w][4]
-   holds its head / head-spans / tail flags. Called by all threads after a CTA barrier. */
+   boundaries becomes a CTA-level piece in global scratch (slot 2j for a piece that continues a
+   segment of the previous group, 2j + 1 for one that starts in group j). Without arrival counters
+   (tk.arrive == nullptr) the tail pieces are listed for the combine kernel. With them, the CTA finds
+   the groups j0..j1 of the segment, publishes its piece (fence, then one atomic increment of the
+   segment's counter) and, if its increment was the last of the j1 - j0 + 1, records the segment in
+   duty[slot] = {1, j0, pieces, key} for finish_segments. piece_at(w, slot) is warp w's head (slot
+   0) or tail (slot 1) piece in shared memory, [REGS][32] doubles; meta[w][4] holds its head /
+   head-spans / tail flags. Called by all threads after a CTA barrier. */
 template <int MT, int NT, typename PieceAt>
 __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int sub, int* __restrict__ seglist,
-  const int* meta, int W, PieceAt piece_at) {
+  const int* meta, int W, PieceAt piece_at, int (*duty)[4]) {
   constexpr int REGS = MT * NT * 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub = tk.nsub;
+  if (threadIdx.x < 8) duty[threadIdx.x >> 2][threadIdx.x & 3] = 0;
+  __syncthreads();
   for (int start = 0; start < 2; ++start) {
     const bool from_head = (0 == start);
     if (from_head && 0 != warp) continue;
@@ -149,19 +214,36 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
       spans = (0 != meta[cur * 4 + 1]);
     }
     const int c_first = group * W + warp; /* chunk where this chain starts */
+    /* the chain's segment: the CTA's first key (head chain) or the last key of its first chunk */
+    const unsigned key = from_head ? tk.keys[(size_t)group * W * L] : tk.keys[min((c_first + 1) * L, S) - 1];
     if (from_head || spans) { /* the segment crosses a CTA boundary: CTA-level piece */
       const int slot = from_head ? 2 * group : 2 * group + 1;
       double* const dst = tk.pieces + ((size_t)slot * nsub + sub) * REGS * 32 + lane;
 #pragma unroll
       for (int r = 0; r < REGS; ++r) dst[r * 32] = sum[r];
-      if (!from_head && 0 == sub && 0 == lane) {
-        const int slotidx = atomicAdd(seglist, 1);
-        seglist[1 + slotidx] = seg_tag(tk.sid, group);
+      if (nullptr == tk.arrive) {
+        if (!from_head && 0 == sub && 0 == lane) {
+          const int slotidx = atomicAdd(seglist, 1);
+          seglist[1 + slotidx] = seg_tag(tk.sid, group);
+        }
+      }
+      else {
+        int j0, j1;
+        segment_groups(tk, group, key, from_head, spans, j0, j1);
+        __threadfence(); /* the piece is visible device-wide before the arrival */
+        __syncwarp();
+        int last = 0;
+        if (0 == lane) last = (atomicAdd(tk.arrive + (size_t)j0 * nsub + sub, 1) == j1 - j0) ? 1 : 0;
+        if (0 != __shfl_sync(0xFFFFFFFFu, last, 0) && 0 == lane) {
+          int* const d = duty[from_head ? 0 : 1];
+          d[1] = j0;
+          d[2] = j1 - j0 + 1;
+          d[3] = (int)key;
+          d[0] = 1;
+        }
       }
     }
     else {
-      const int p1 = min((c_first + 1) * L, S);
-      const unsigned key = tk.keys[p1 - 1]; /* a tail piece belongs to the last segment of its chunk */
       double tile[MT][NT][2];
 #pragma unroll
       for (int i = 0; i < MT; ++i)
@@ -174,6 +256,73 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
       tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
       commit_tile<MT, NT>(tk.c, (size_t)key - 1, tile, tk.m, tk.n, g, t, tl, tk.alpha);
     }
+  }
+}
+
+/* Combines the segments whose last piece this CTA published (duty, filled by cta_merge): the
+   segment's pieces are the tail piece of its first group j0 and the head pieces of the groups after
+   it; warp w sums pieces w, w + W, ... in order, the warps' partials are added in warp order in red
+   ([W - 1][REGS][32] doubles of shared memory no longer in use), and warp 0 writes the block once.
+   The summation tree depends only on the number of pieces and W: the result is reproducible. Called
+   by all threads after a CTA barrier that follows cta_merge; ends with a barrier. */
+template <int MT, int NT>
+__device__ __forceinline__ void finish_segments(const StackTask& tk, int sub, int (*duty)[4], double* red) {
+  constexpr int REGS = MT * NT * 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5, g = lane >> 2, t = lane & 3;
+  const int nsub = tk.nsub;
+  for (int d = 0; d < 2; ++d) {
+    if (0 == duty[d][0]) continue; /* uniform: shared memory read after a barrier */
+    const int j0 = duty[d][1], np = duty[d][2];
+    const unsigned key = (unsigned)duty[d][3];
+    __threadfence(); /* the other groups' pieces were published before their arrivals */
+    double acc[REGS];
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
+    int q = warp;
+    for (; q + W < np; q += 2 * W) { /* two pieces in flight per step */
+      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q), s1 = 2 * (j0 + q + W);
+      const double* const p0 = tk.pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
+      const double* const p1 = tk.pieces + ((size_t)s1 * nsub + sub) * REGS * 32 + lane;
+      double v0[REGS], v1[REGS];
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) {
+        v0[r] = __ldcg(p0 + r * 32);
+        v1[r] = __ldcg(p1 + r * 32);
+      }
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += v0[r];
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += v1[r];
+    }
+    if (q < np) {
+      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q);
+      const double* const p0 = tk.pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += __ldcg(p0 + r * 32);
+    }
+    if (0 != warp) {
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) red[((warp - 1) * REGS + r) * 32 + lane] = acc[r];
+    }
+    __syncthreads();
+    if (0 == warp) {
+      for (int w2 = 0; w2 < W - 1; ++w2) {
+#pragma unroll
+        for (int r = 0; r < REGS; ++r) acc[r] += red[(w2 * REGS + r) * 32 + lane];
+      }
+      Tile<MT, NT> tl;
+      tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
+      double tile[MT][NT][2];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          tile[i][j][0] = acc[(i * NT + j) * 2 + 0];
+          tile[i][j][1] = acc[(i * NT + j) * 2 + 1];
+        }
+      commit_tile<MT, NT>(tk.c, (size_t)key - 1, tile, tk.m, tk.n, g, t, tl, tk.alpha);
+    }
+    __syncthreads();
   }
 }
 
@@ -328,15 +477,19 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
     }
   }
   __syncthreads();
+  __shared__ int duty[2][4];
   cta_merge<MT, NT>(tk, group, sub, seglist, meta, W,
-    [&](int w, int slot) -> const double* { return sp + ((size_t)(w * 2 + slot) * REGS) * 32; });
+    [&](int w, int slot) -> const double* { return sp + ((size_t)(w * 2 + slot) * REGS) * 32; }, duty);
   __syncthreads();
+  if (nullptr != tk.arrive) finish_segments<MT, NT>(tk, sub, duty, sp);
 }
 
 template <int M_, int N_, int K_, int MT, int NT, int KP>
 __global__ void __launch_bounds__(128, smm_min_blocks(MT, NT))
   xs_smm_dmma_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, const unsigned* __restrict__ err) {
   extern __shared__ double smem[];
+  pdl_wait();
+  pdl_trigger();
   if (0 != *(volatile const unsigned*)err) return; /* the grouping failed: write nothing */
   const int group = blockIdx.x / tk.nsub, sub = blockIdx.x - group * tk.nsub;
   smm_item<M_, N_, K_, MT, NT, KP>(tk, group, sub, seglist, smem);
@@ -408,6 +561,8 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
   constexpr int MT = G::MT, NT = G::NT, REGS = G::REGS, KS = G::KS;
   constexpr unsigned FULL = 0xFFFFFFFFu;
   extern __shared__ __align__(128) unsigned char smraw[];
+  pdl_wait();
+  pdl_trigger();
   if (0 != *(volatile const unsigned*)err) return;
   const int W = blockDim.x >> 5;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
@@ -586,9 +741,14 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
     if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
     return;
   }
+  __shared__ int duty[2][4];
   cta_merge<MT, NT>(tk, group, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
     return (const double*)(smraw + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
-  });
+  }, duty);
+  if (nullptr != tk.arrive) {
+    __syncthreads();
+    finish_segments<MT, NT>(tk, 0, duty, (double*)smraw);
+  }
 }
 
 /* Task table of a batch (kernel parameter: read through the constant bank). */
@@ -631,6 +791,8 @@ __global__ void __launch_bounds__(128, batch_group_min_blocks(GRP))
     const unsigned* __restrict__ err) {
   extern __shared__ double smem[];
   __shared__ int s_item;
+  pdl_wait();
+  pdl_trigger();
   if (0 != *(volatile const unsigned*)err) return;
   for (;;) {
     if (0 == threadIdx.x) s_item = (int)atomicAdd(queue, 1u);
@@ -742,6 +904,7 @@ __global__ void __launch_bounds__(32 * kCombineWarps)
   xs_smm_combine_kernel(const __grid_constant__ StackTask tk, int W, const int* __restrict__ seglist,
     const unsigned* __restrict__ err) {
   extern __shared__ double red[]; /* [CW - 1][REGS][32] */
+  pdl_wait();
   if (0 != *(volatile const unsigned*)err) return;
   const int count = seglist[0];
   for (int w = blockIdx.x; w < count * tk.nsub; w += gridDim.x) {
@@ -763,6 +926,7 @@ __global__ void __launch_bounds__(32 * kCombineWarps)
   xs_smm_combine_batch_kernel(const __grid_constant__ BatchTasks bt, int W, const int* __restrict__ seglist,
     const unsigned* __restrict__ err) {
   extern __shared__ double red[];
+  pdl_wait();
   if (0 != *(volatile const unsigned*)err) return;
   const int count = seglist[0];
   for (int li = blockIdx.x; li < count; li += gridDim.x) {
@@ -796,7 +960,7 @@ struct SmmPlan {
   int nsub_m, nsub_n, nsub, nchunks, L, W, ngroups;
   int no_combine; /* the stack kernel only: CTA-crossing pieces are combined by the caller */
   size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces;
-  size_t off_sort, total;
+  size_t off_arrive, off_sort, total;
 };
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -848,6 +1012,8 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   off = align_up(off + sizeof(int) * ((size_t)pl->ngroups + 1), 256);
   pl->off_pieces = off;
   off = align_up(off + sizeof(double) * (size_t)2 * pl->ngroups * pl->nsub * (mt * nt * 2) * 32, 256);
+  pl->off_arrive = off;
+  off = align_up(off + sizeof(int) * (size_t)pl->ngroups * pl->nsub, 256);
   pl->off_sort = off;
   off = align_up(off + xs_stack_sort_scratch_bytes(S), 256);
   pl->total = off;
@@ -866,8 +1032,7 @@ cudaError_t launch_combine(const SmmPlan& pl, const StackTask& tk, const int* se
     csmem_set = 1;
   }
   void* prof = xs_profile_begin(s);
-  xs_smm_combine_kernel<MT, NT><<<cgrid, 32 * kCombineWarps, csmem, s>>>(tk, pl.W, seglist, err);
-  const cudaError_t r = cudaGetLastError();
+  const cudaError_t r = pdl_launch(xs_smm_combine_kernel<MT, NT>, cgrid, 32 * kCombineWarps, csmem, s, tk, pl.W, seglist, err);
   xs_profile_end(prof, "combine", 0.0, 0.0, s);
   return r;
 }
@@ -888,12 +1053,11 @@ cudaError_t launch_dmma(const SmmPlan& pl, const StackTask& tk, int* seglist, co
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, 32 * pl.W, smem);
   }
   void* prof = xs_profile_begin(s);
-  xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP><<<pl.ngroups * pl.nsub, 32 * pl.W, smem, s>>>(tk, seglist, err);
-  r = cudaGetLastError();
+  r = pdl_launch(xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, pl.ngroups * pl.nsub, 32 * pl.W, smem, s, tk, seglist, err);
   if (cudaSuccess != r) return r;
   const double m = tk.m, n = tk.n, k = tk.k;
   xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
-  return pl.no_combine ? cudaSuccess : launch_combine<MT, NT>(pl, tk, seglist, err, s);
+  return (pl.no_combine || nullptr != tk.arrive) ? cudaSuccess : launch_combine<MT, NT>(pl, tk, seglist, err, s);
 }
 
 /* The staged kernel of one block shape with an R-deep ring per warp, then the combine. */
@@ -912,12 +1076,12 @@ cudaError_t launch_staged(const SmmPlan& pl, const StackTask& tk, int* seglist, 
   if (nullptr != occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_staged_kernel<M_, N_, K_, R>, 32 * pl.W, smem);
   if (1 != pl.nsub) return cudaErrorInvalidValue; /* one warp tile per C block */
   void* prof = xs_profile_begin(s);
-  xs_smm_staged_kernel<M_, N_, K_, R><<<pl.ngroups, 32 * pl.W, smem, s>>>(tk, seglist, (unsigned*)err, xs_device_error_ptr());
-  r = cudaGetLastError();
+  r = pdl_launch(xs_smm_staged_kernel<M_, N_, K_, R>, pl.ngroups, 32 * pl.W, smem, s, tk, seglist, (unsigned*)err,
+    xs_device_error_ptr());
   if (cudaSuccess != r) return r;
   const double m = M_, n = N_, k = K_;
   xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
-  return pl.no_combine ? cudaSuccess : launch_combine<G::MT, G::NT>(pl, tk, seglist, err, s);
+  return (pl.no_combine || nullptr != tk.arrive) ? cudaSuccess : launch_combine<G::MT, G::NT>(pl, tk, seglist, err, s);
 }
 
 /* Runtime-shape kernels: any (m, n, k), warp sub-tile MT x NT, KP in {2, 4}. */
@@ -1010,8 +1174,7 @@ cudaError_t batch_smm(const BatchTasks& bt, int* seglist, unsigned* queue, const
   if (cudaSuccess != r) return r;
   const int grid = max(1, min(bt.nitems, max(1, occ) * xs_sm_count()));
   void* prof = xs_profile_begin(s);
-  xs_smm_batch_kernel<GRP><<<grid, 32 * kBatchW, batch_smem_bytes(GRP), s>>>(bt, seglist, queue, err);
-  r = cudaGetLastError();
+  r = pdl_launch(xs_smm_batch_kernel<GRP>, grid, 32 * kBatchW, batch_smem_bytes(GRP), s, bt, seglist, queue, err);
   xs_profile_end(prof, "smm_batch", flops, bytes, s);
   return r;
 }
@@ -1023,9 +1186,8 @@ cudaError_t batch_combine(const BatchTasks& bt, int ngroups_total, int* seglist,
   if (cudaSuccess != r) return r;
   void* prof = xs_profile_begin(s);
   const int cgrid = max(1, min(ngroups_total, 2 * xs_sm_count()));
-  xs_smm_combine_batch_kernel<X><<<cgrid, 32 * kCombineWarps, sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32, s>>>(
-    bt, kBatchW, seglist, err);
-  r = cudaGetLastError();
+  r = pdl_launch(xs_smm_combine_batch_kernel<X>, cgrid, 32 * kCombineWarps, sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32,
+    s, bt, kBatchW, seglist, err);
   xs_profile_end(prof, "combine_batch", 0.0, 0.0, s);
   return r;
 }
@@ -1338,9 +1500,10 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   unsigned long long* const vals_out = (unsigned long long*)(base + pl.off_vals_out);
   int* const seglist = (int*)(base + pl.off_seglist);
   void* const sort_scratch = base + pl.off_sort;
+  int* const arrive = (int*)(base + pl.off_arrive);
   void* prof = xs_profile_begin(s);
   const int r = xs_stack_group_ex(dev_stack, S, format, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, seglist,
-    sort_scratch, s);
+    arrive, pl.ngroups * pl.nsub, sort_scratch, s);
   if (0 != r) return r;
   xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
   StackTask tk = {};
@@ -1360,6 +1523,7 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   tk.ngroups = pl.ngroups;
   tk.nsub_n = pl.nsub_n;
   tk.nsub = pl.nsub;
+  tk.arrive = arrive; /* CTA-crossing segments are combined inside the stack kernel */
   const launch_fn_t fn = find_launcher(m, n, k, prm);
   return (int)fn(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
 }
@@ -1392,7 +1556,7 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
   if (0 != r) return r;
   void* prof = xs_profile_begin(s);
   xs_sort_batch_t sb;
-  sb.nstacks = 0;
+  memset(&sb, 0, sizeof(sb));
   int tiles = 0;
   const int launch_tiles = xs_sort_launch_tiles(), tile_entries = xs_sort_tile_entries(1);
   for (int q = 0; q <= bp.nparts; ++q) {

@@ -175,6 +175,9 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     if (nullptr != stamps && 0 == threadIdx.x) stamps[tile * 8 + (slot)] = global_ns(); \
   } while (0)
   XS_STAMP(0);
+  /* the stack kernel launched after this one may be scheduled now (programmatic dependent launch);
+     it waits for this kernel's completion before it reads the grouped stack */
+  asm volatile("griddepcontrol.launch_dependents;" :::);
 
   /* phase 0: load + bucket statistics of this stack */
   {
@@ -233,6 +236,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
       }
       if (0 == tile && nullptr != seglist) seglist[0] = 0;
     }
+    for (int i = tile * kSortThreads + (int)threadIdx.x; i < desc.nzero; i += ntiles_all * kSortThreads) desc.zero[i] = 0;
     XS_STAMP(1);
     if (!grid_sync(ctl)) return;
     XS_STAMP(2);
@@ -520,13 +524,16 @@ int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned lon
 
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
-  return xs_stack_group_ex(dev_stack, S, 0, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, stream);
+  return xs_stack_group_ex(dev_stack, S, 0, k0, v0, k1, v1, kout, vout, seglist, nullptr, 0, sort_scratch, stream);
 }
 
 int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned* k0, unsigned long long* v0, unsigned* k1,
-  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
+  void* stream) {
   xs_sort_batch_t d;
   memset(&d, 0, sizeof(d));
+  d.zero = zero;
+  d.nzero = (nullptr != zero) ? nzero : 0;
   d.nstacks = 1;
   d.stack[0] = dev_stack;
   d.format[0] = format;
