@@ -161,8 +161,9 @@ int xs_stack_group_fits(const xs_sort_batch_t* desc);
     (xs_sort_clear_ctl) before the first launch of the call. */
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
-/** As xs_stack_group, for either parameter format; also zeroes nzero ints at zero (nullptr: none). */
-int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned* k0, unsigned long long* v0, unsigned* k1,
+/** As xs_stack_group, for either parameter format; also zeroes nzero ints at zero (nullptr: none).
+    blk > 0: the C block size (blocks of the stack do not overlap), which spares the gcd statistics. */
+int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
   void* stream);
 int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,

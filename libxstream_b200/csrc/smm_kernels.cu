@@ -1502,8 +1502,8 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   void* const sort_scratch = base + pl.off_sort;
   int* const arrive = (int*)(base + pl.off_arrive);
   void* prof = xs_profile_begin(s);
-  const int r = xs_stack_group_ex(dev_stack, S, format, keys_in, vals_in, keys_tmp, vals_tmp, keys_out, vals_out, seglist,
-    arrive, pl.ngroups * pl.nsub, sort_scratch, s);
+  const int r = xs_stack_group_ex(dev_stack, S, format, (unsigned)(m * n), keys_in, vals_in, keys_tmp, vals_tmp, keys_out,
+    vals_out, seglist, arrive, pl.ngroups * pl.nsub, sort_scratch, s);
   if (0 != r) return r;
   xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
   StackTask tk = {};

@@ -16,6 +16,7 @@
  * error word, and returns instead of hanging.
  */
 #include "internal.h"
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -425,6 +426,251 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
 #undef XS_STAMP
 }
 
+/* ------------------------------------------------------------------ one-cluster grouping (small stacks) */
+
+/* Largest cluster the one-cluster grouping uses (16: non-portable size, one GPC) and the most entries
+   it takes (16 CTAs x 2048, or 8 CTAs x 4096 where clusters of 16 are not available). */
+constexpr int kClusterMax = 16;
+constexpr int kClusterEntries = kClusterMax * kSortThreads * 8;
+
+/* Bucket floor(x / d) from a double reciprocal with a one-step correction (exact for x < 2^32). */
+__device__ __forceinline__ unsigned bucket_floor(unsigned x, unsigned d, double inv_d) {
+  unsigned q = (unsigned)((double)x * inv_d);
+  const unsigned long long p = (unsigned long long)q * d;
+  if (p > x) --q;
+  else if (p + d <= x) ++q;
+  return q;
+}
+
+/* Grouping of one stack of at most kClusterEntries entries by ONE thread-block cluster: the same
+   stable LSD counting sort as xs_stack_group_kernel (same tiles, digits and ranks, hence the same
+   output), with the cluster's CTAs exchanging statistics and counts by pushing them into each
+   other's shared memory between cluster barriers: no grid-wide barrier, global histogram table or
+   atomic statistics, and no memset (CTA 0 clears the error word and the segment list). Bucket ids:
+   with blk > 0 (the C block size: blocks of one stack do not overlap, so distinct blocks lie at least
+   blk apart) id = (c - cmin) / blk, which needs only the minimum and maximum; with blk == 0 the gcd
+   of the offset differences divides them exactly, as in xs_stack_group_kernel. Per pass, each warp
+   counts its entries per digit (match masks, one count per distinct digit), the per-digit totals of
+   the CTA follow from the per-warp counts, the digits' owner CTAs (digit d: CTA d / DR) turn the
+   counts of all CTAs into write positions and push them back, and every warp places its entries in
+   stack order. Cluster barriers are hardware barriers of co-scheduled CTAs and cannot hang. */
+template <int E>
+__global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(const int* __restrict__ stack, int S, int format,
+  unsigned blk, unsigned* __restrict__ k0, unsigned long long* __restrict__ v0, unsigned* __restrict__ k1,
+  unsigned long long* __restrict__ v1, unsigned* __restrict__ kout, unsigned long long* __restrict__ vout,
+  int* __restrict__ seglist, int* __restrict__ zero, int nzero, SortCtl* ctl) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned short s_wc_raw[]; /* [kSortWarps][kRadix] (dynamic: static memory is full) */
+  unsigned short (*const s_wc)[kRadix] = reinterpret_cast<unsigned short (*)[kRadix]>(s_wc_raw);
+  __shared__ int s_hist[kRadix]; /* this CTA's digit totals */
+  __shared__ int s_gath[kRadix]; /* [q][dl]: CTA q's count of owned digit dl, pushed by q */
+  __shared__ int s_base[kRadix]; /* digit write positions of this CTA, pushed by the digits' owners */
+  __shared__ int s_wsum[kSortWarps];
+  __shared__ unsigned s_red[3][kSortWarps];
+  __shared__ unsigned s_stat[kClusterMax][3]; /* cmin, cmax, gcd of every CTA, pushed by each */
+  __shared__ int s_slice[kClusterMax];          /* digit-slice totals of every owner, pushed by each */
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
+  asm volatile("griddepcontrol.launch_dependents;" :::);
+  /* every CTA of the cluster must be running before another one writes into its shared memory: arrive
+     now, wait before the first push (the stack loads overlap the barrier) */
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+  const int pstride = (0 != format) ? 6 : 3, pbase = (0 != format) ? 3 : 0, pone = (0 != format) ? 1 : 0;
+  const int T = kSortThreads * E;
+  const int t0 = min(S, rank * T), t1 = min(S, t0 + T);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int w0 = min(t1, t0 + warp * 32 * E), w1 = min(t1, w0 + 32 * E);
+  unsigned key[E];
+  unsigned long long val[E];
+  if (0 == rank && 0 == threadIdx.x) {
+    ctl->err = 0u;
+    if (nullptr != seglist) seglist[0] = 0;
+  }
+  for (int i = rank * kSortThreads + (int)threadIdx.x; i < nzero; i += ncta * kSortThreads) zero[i] = 0;
+  { /* load + statistics */
+    unsigned lo = 0xFFFFFFFFu, hi = 0u, gg = 0u;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int i = w0 + lane + 32 * r;
+      key[r] = 0u;
+      val[r] = 0ull;
+      if (i < w1) {
+        const int* const e = stack + (size_t)pstride * i + pbase;
+        const int a = e[0] + pone, b = e[1] + pone;
+        key[r] = (unsigned)(e[2] + pone);
+        val[r] = (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32);
+        lo = min(lo, key[r]);
+        hi = max(hi, key[r]);
+      }
+    }
+    if (0 == blk) { /* gcd of the differences to the stack's first offset */
+      const unsigned c0 = (unsigned)(stack[pbase + 2] + pone);
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        if (w0 + lane + 32 * r < w1) gg = gcd_acc(gg, (key[r] > c0) ? key[r] - c0 : c0 - key[r]);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) gg = gcd_acc(gg, __shfl_xor_sync(0xffffffffu, gg, o));
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if (0 == lane) {
+      s_red[0][warp] = lo;
+      s_red[1][warp] = hi;
+      s_red[2][warp] = gg;
+    }
+    __syncthreads();
+    if (0 == warp) {
+      lo = (lane < kSortWarps) ? s_red[0][lane] : 0xFFFFFFFFu;
+      hi = (lane < kSortWarps) ? s_red[1][lane] : 0u;
+      lo = __reduce_min_sync(0xffffffffu, lo);
+      hi = __reduce_max_sync(0xffffffffu, hi);
+      if (0 == lane && 0 == blk) {
+        for (int w = 1; w < kSortWarps; ++w) gg = gcd_acc(gg, s_red[2][w]);
+      }
+      gg = __shfl_sync(0xffffffffu, gg, 0);
+    }
+    asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
+    if (0 == warp && lane < ncta) { /* push this CTA's statistics to every CTA of the cluster */
+      unsigned* const st = cluster.map_shared_rank(&s_stat[rank][0], lane);
+      st[0] = lo;
+      st[1] = hi;
+      st[2] = gg;
+    }
+  }
+  cluster.sync();
+  unsigned cmin = 0xFFFFFFFFu, cmax = 0u, g = blk;
+  for (int q = 0; q < ncta; ++q) { /* every thread combines the cluster's statistics (same order) */
+    cmin = min(cmin, s_stat[q][0]);
+    cmax = max(cmax, s_stat[q][1]);
+    if (0 == blk) g = gcd_acc(g, s_stat[q][2]);
+  }
+  const unsigned nb = (0 == g) ? 1u : (cmax - cmin) / g + 1u;
+  const double inv_g = (0 == g) ? 0.0 : 1.0 / (double)g;
+  int bits = 0;
+  while (bits < 32 && (nb - 1u) >> bits) ++bits;
+  const int passes = (bits + kRadixBits - 1) / kRadixBits;
+  if (0 == passes) { /* a single C block: already grouped, keep stack order */
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int i = w0 + lane + 32 * r;
+      if (i < w1) {
+        kout[i] = key[r];
+        vout[i] = val[r];
+      }
+    }
+  }
+  const int rb = (0 == passes) ? 0 : (bits + passes - 1) / passes, R = 1 << rb;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int shift = pass * rb;
+    const bool last = (pass + 1 == passes);
+    unsigned* const kdst = last ? kout : ((0 == (pass & 1)) ? k1 : k0);
+    unsigned long long* const vdst = last ? vout : ((0 == (pass & 1)) ? v1 : v0);
+    int dig[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      dig[r] = (w0 + lane + 32 * r < w1) ? (int)((bucket_floor(key[r] - cmin, g, inv_g) >> shift) & (R - 1)) : kRadix;
+    }
+    /* (a) per-warp digit counts (the leader of each group of equal digits adds the group's size),
+       then per digit: exclusive prefix over the warps in place, CTA total */
+    for (int j = threadIdx.x; j < kSortWarps * R / 8; j += blockDim.x) { /* 8 counters per 16-byte store */
+      const int w = j / (R / 8), d8 = j - w * (R / 8);
+      if (R >= 8) reinterpret_cast<uint4*>(&s_wc[w][0])[d8] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (R < 8 && (int)threadIdx.x < kSortWarps * R) s_wc[threadIdx.x / R][threadIdx.x % R] = 0;
+    __syncthreads();
+    unsigned peers[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      peers[r] = __match_any_sync(0xffffffffu, dig[r]);
+      if (kRadix != dig[r] && 0 == __popc(peers[r] & ((1u << lane) - 1u))) {
+        s_wc[warp][dig[r]] += (unsigned short)__popc(peers[r]);
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    for (int dd = threadIdx.x; dd < R; dd += blockDim.x) {
+      int run = 0;
+#pragma unroll
+      for (int w2 = 0; w2 < kSortWarps; ++w2) {
+        const int c = s_wc[w2][dd];
+        s_wc[w2][dd] = (unsigned short)run;
+        run += c;
+      }
+      s_hist[dd] = run;
+    }
+    __syncthreads();
+    /* (b) digit bases. Digits are owned in slices of DR by the CTAs (digit d by CTA d / DR). Every
+       exchange is a push into another CTA's shared memory followed by a cluster barrier: counts to
+       the owners, slice totals to all, then each (digit, CTA) base to that CTA. */
+    const int DR = (R + ncta - 1) / ncta;
+    for (int d = threadIdx.x; d < R; d += blockDim.x) {
+      const int q = d / DR;
+      *cluster.map_shared_rank(&s_gath[rank * DR + (d - q * DR)], q) = s_hist[d];
+    }
+    cluster.sync();
+    constexpr int PER = kRadix / kSortThreads;
+    const int per = (DR + kSortThreads - 1) / kSortThreads;
+    int tot[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) { /* owned digit dl: prefix over the CTAs in place, total */
+      const int dl = threadIdx.x * per + j;
+      int run = 0;
+      if (j < per && dl < DR && rank * DR + dl < R) {
+        for (int q = 0; q < ncta; ++q) {
+          const int x = s_gath[q * DR + dl];
+          s_gath[q * DR + dl] = run;
+          run += x;
+        }
+      }
+      tot[j] = run;
+    }
+    int slice = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) slice += tot[j];
+    block_exscan<PER>(tot, s_wsum);
+    if (kSortThreads - 1 == (int)threadIdx.x) { /* the last thread's exclusive start + its own sum */
+      for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(&s_slice[rank], q) = tot[0] + slice;
+    }
+    cluster.sync();
+    int slice_off = 0;
+    for (int q = 0; q < rank; ++q) slice_off += s_slice[q];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int dl = threadIdx.x * per + j;
+      const int d = rank * DR + dl;
+      if (j < per && dl < DR && d < R) {
+        for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(&s_base[d], q) = slice_off + tot[j] + s_gath[q * DR + dl];
+      }
+    }
+    cluster.sync();
+    /* (c) stable scatter in stack order: CTA base + warp offset + rank within the warp */
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int rank_w = __popc(peers[r] & ((1u << lane) - 1u));
+      if (kRadix != dig[r]) {
+        const int pos = s_base[dig[r]] + s_wc[warp][dig[r]] + rank_w;
+        kdst[pos] = key[r];
+        vdst[pos] = val[r];
+      }
+      __syncwarp();
+      if (kRadix != dig[r] && 0 == rank_w) s_wc[warp][dig[r]] += (unsigned short)__popc(peers[r]);
+      __syncwarp();
+    }
+    if (!last) {
+      cluster.sync(); /* this pass's output is visible to the whole cluster */
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const int i = w0 + lane + 32 * r;
+        if (i < w1) {
+          key[r] = __ldcg(kdst + i);
+          val[r] = __ldcg(vdst + i);
+        }
+      }
+    }
+  }
+}
+
 /* Entries per thread kept in registers: 8 (tiles of 2048) or 16 (tiles of 4096). */
 constexpr int kTileSmall = kSortThreads * 8, kTileLarge = kSortThreads * 16;
 
@@ -484,6 +730,42 @@ int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long*
     args, 0, s);
 }
 
+/* Launches the one-cluster grouping with ncta CTAs (a power of two <= kClusterMax) of E entries per
+   thread. Returns cudaErrorNotSupported, launching nothing, when the device cannot run a cluster of
+   that size. */
+int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, SortCtl* ctl, int ncta,
+  int E, cudaStream_t s) {
+  static int ok[2][kClusterMax + 1]; /* per E and cluster size: 0 unknown, 1 supported, -1 not */
+  auto kernel = (16 == E) ? xs_stack_group_cluster_kernel<16> : xs_stack_group_cluster_kernel<8>;
+  int* const okp = &ok[(16 == E) ? 1 : 0][ncta];
+  const size_t smem = sizeof(unsigned short) * kSortWarps * kRadix;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ncta);
+  cfg.blockDim = dim3(kSortThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)ncta;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (0 == *okp) {
+    int nclusters = 0;
+    cudaError_t r = cudaSuccess;
+    /* static + dynamic shared memory exceed the default 48 KB per CTA */
+    r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaSuccess == r && ncta > 8) r = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (cudaSuccess == r) r = cudaOccupancyMaxActiveClusters(&nclusters, kernel, &cfg);
+    *okp = (cudaSuccess == r && 0 < nclusters) ? 1 : -1;
+    if (cudaSuccess != r) (void)cudaGetLastError(); /* not sticky: clear it */
+  }
+  if (0 > *okp) return (int)cudaErrorNotSupported;
+  return (int)cudaLaunchKernelEx(&cfg, kernel, stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero, ctl);
+}
+
 }  // namespace
 
 extern "C" {
@@ -524,12 +806,23 @@ int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned lon
 
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
-  return xs_stack_group_ex(dev_stack, S, 0, k0, v0, k1, v1, kout, vout, seglist, nullptr, 0, sort_scratch, stream);
+  return xs_stack_group_ex(dev_stack, S, 0, 0u, k0, v0, k1, v1, kout, vout, seglist, nullptr, 0, sort_scratch, stream);
 }
 
-int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned* k0, unsigned long long* v0, unsigned* k1,
+int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
   void* stream) {
+  if (0 < S && S <= kClusterEntries) { /* one cluster: tiles of 2048 entries, else half as many of 4096 */
+    int ncta = 1;
+    while (ncta * kSortThreads * 8 < S) ncta <<= 1;
+    int r = cluster_group_launch(dev_stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero,
+      (SortCtl*)sort_scratch, ncta, 8, (cudaStream_t)stream);
+    if (cudaErrorNotSupported == r && 1 < ncta) {
+      r = cluster_group_launch(dev_stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero,
+        (SortCtl*)sort_scratch, ncta / 2, 16, (cudaStream_t)stream);
+    }
+    if (cudaErrorNotSupported != r) return r; /* else: the cooperative kernel below */
+  }
   xs_sort_batch_t d;
   memset(&d, 0, sizeof(d));
   d.zero = zero;

@@ -291,3 +291,16 @@ def test_irregular_c_offsets_multipass_sort(acc):
     err = np.abs(got - ref).max() / np.abs(ref).max()
     assert err <= TOL
     del case2
+
+
+@pytest.mark.parametrize("S", [2048, 2049, 16385, 32768, 32769])
+def test_grouping_cluster_and_cooperative_sizes(acc, S):
+    """Stacks of up to 16 tiles of 2048 entries are grouped by one thread-block cluster, larger ones by
+    the cooperative kernel; both sides of each size boundary agree with the oracle and are bitwise
+    reproducible."""
+    A, stream = acc
+    case = W.stack_case(23, 23, 23, S, 500, 500, 300, seed=S)
+    r1 = run_device(A, stream, case)
+    r2 = run_device(A, stream, case)
+    assert np.array_equal(r1, r2)
+    assert oracle.block_relerr(r1, oracle_c(case), 529) <= TOL
