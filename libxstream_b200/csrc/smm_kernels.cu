@@ -142,6 +142,13 @@ struct StackTask {
 /* Segment-list entry: stack index (high 8 bits) and CTA group (low 24 bits). */
 __device__ __forceinline__ int seg_tag(int sid, int group) { return (sid << 24) | group; }
 
+/* Pieces per first-level combine of a long CTA-crossing segment. */
+constexpr int kFan = 8;
+
+/* Scratch slot of piece q of the segment whose first group is j0: the tail piece of group j0 (q = 0),
+   else the head piece of group j0 + q. */
+__device__ __forceinline__ int piece_slot(int j0, int q) { return (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q); }
+
 /* Groups j0 <= j <= j1 (j0, j1 returned) that hold entries of the segment with key x, for a segment
    that the CTA group j holds and that crosses j's first boundary (head: entry j*Lc - 1 has key x)
    and/or its last one (tail: entry (j+1)*Lc has key x). Keys are sorted, so the boundaries a segment
@@ -183,18 +190,22 @@ __device__ __forceinline__ void segment_groups(const StackTask& tk, int j, unsig
    boundaries becomes a CTA-level piece in global scratch (slot 2j for a piece that continues a
    segment of the previous group, 2j + 1 for one that starts in group j). Without arrival counters
    (tk.arrive == nullptr) the tail pieces are listed for the combine kernel. With them, the CTA finds
-   the groups j0..j1 of the segment, publishes its piece (fence, then one atomic increment of the
-   segment's counter) and, if its increment was the last of the j1 - j0 + 1, records the segment in
-   duty[slot] = {1, j0, pieces, key} for finish_segments. piece_at(w, slot) is warp w's head (slot
-   0) or tail (slot 1) piece in shared memory, [REGS][32] doubles; meta[w][4] holds its head /
-   head-spans / tail flags. Called by all threads after a CTA barrier. */
+   the groups j0..j1 of the segment (its np = j1 - j0 + 1 pieces, piece q from group j0 + q) and
+   publishes its piece (fence, then one atomic increment): a segment of at most kFan pieces has one
+   counter, and the CTA whose increment completes it combines all pieces; a longer one is combined
+   in two levels, kFan consecutive pieces per first-level counter (the CTA completing one sums them
+   and then arrives at the segment's counter) and the first-level sums at the end. The CTA records
+   what it completed in duty[slot] = {1, j0, np, key, level, first-level group} for finish_segments.
+   piece_at(w, slot) is warp w's head (slot 0) or tail (slot 1) piece in shared memory, [REGS][32]
+   doubles; meta[w][4] holds its head / head-spans / tail flags. Called by all threads after a CTA
+   barrier. */
 template <int MT, int NT, typename PieceAt>
 __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int sub, int* __restrict__ seglist,
-  const int* meta, int W, PieceAt piece_at, int (*duty)[4]) {
+  const int* meta, int W, PieceAt piece_at, int (*duty)[6]) {
   constexpr int REGS = MT * NT * 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub = tk.nsub;
-  if (threadIdx.x < 8) duty[threadIdx.x >> 2][threadIdx.x & 3] = 0;
+  if (threadIdx.x < 12) duty[threadIdx.x / 6][threadIdx.x % 6] = 0;
   __syncthreads();
   for (int start = 0; start < 2; ++start) {
     const bool from_head = (0 == start);
@@ -230,15 +241,22 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
       else {
         int j0, j1;
         segment_groups(tk, group, key, from_head, spans, j0, j1);
+        const int np = j1 - j0 + 1, q = group - j0;
+        const int level = (np <= kFan) ? 2 : 1, i1 = q / kFan;
+        const int target = (2 == level) ? np : min(kFan, np - i1 * kFan);
+        int* const counter = (2 == level) ? tk.arrive + (size_t)j0 * nsub + sub
+                                          : tk.arrive + (size_t)tk.ngroups * nsub + (size_t)piece_slot(j0, i1 * kFan) * nsub + sub;
         __threadfence(); /* the piece is visible device-wide before the arrival */
         __syncwarp();
         int last = 0;
-        if (0 == lane) last = (atomicAdd(tk.arrive + (size_t)j0 * nsub + sub, 1) == j1 - j0) ? 1 : 0;
+        if (0 == lane) last = (atomicAdd(counter, 1) == target - 1) ? 1 : 0;
         if (0 != __shfl_sync(0xFFFFFFFFu, last, 0) && 0 == lane) {
           int* const d = duty[from_head ? 0 : 1];
           d[1] = j0;
-          d[2] = j1 - j0 + 1;
+          d[2] = np;
           d[3] = (int)key;
+          d[4] = level;
+          d[5] = i1;
           d[0] = 1;
         }
       }
@@ -259,57 +277,91 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
   }
 }
 
-/* Combines the segments whose last piece this CTA published (duty, filled by cta_merge): the
-   segment's pieces are the tail piece of its first group j0 and the head pieces of the groups after
-   it; warp w sums pieces w, w + W, ... in order, the warps' partials are added in warp order in red
-   ([W - 1][REGS][32] doubles of shared memory no longer in use), and warp 0 writes the block once.
-   The summation tree depends only on the number of pieces and W: the result is reproducible. Called
-   by all threads after a CTA barrier that follows cta_merge; ends with a barrier. */
+/* Sums count pieces, piece i at slot slot_of(i), in a fixed order: warp w takes pieces w, w + W, ...
+   (two in flight), the warps' partials are added in warp order through red ([W - 1][REGS][32]
+   doubles of shared memory no longer in use). The tree depends only on count and W, so the result is
+   reproducible; it is valid in warp 0. Called by all threads; contains a CTA barrier. */
+template <int REGS, typename SlotOf>
+__device__ __forceinline__ void sum_pieces(const StackTask& tk, int sub, int count, SlotOf slot_of, double* red,
+  double (&acc)[REGS]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const int nsub = tk.nsub;
+#pragma unroll
+  for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
+  int q = warp;
+  for (; q + W < count; q += 2 * W) {
+    const double* const p0 = tk.pieces + ((size_t)slot_of(q) * nsub + sub) * REGS * 32 + lane;
+    const double* const p1 = tk.pieces + ((size_t)slot_of(q + W) * nsub + sub) * REGS * 32 + lane;
+    double v0[REGS], v1[REGS];
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) {
+      v0[r] = __ldcg(p0 + r * 32);
+      v1[r] = __ldcg(p1 + r * 32);
+    }
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] += v0[r];
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] += v1[r];
+  }
+  if (q < count) {
+    const double* const p0 = tk.pieces + ((size_t)slot_of(q) * nsub + sub) * REGS * 32 + lane;
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) acc[r] += __ldcg(p0 + r * 32);
+  }
+  if (0 != warp) {
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) red[((warp - 1) * REGS + r) * 32 + lane] = acc[r];
+  }
+  __syncthreads();
+  if (0 == warp) {
+    for (int w2 = 0; w2 < W - 1; ++w2) {
+#pragma unroll
+      for (int r = 0; r < REGS; ++r) acc[r] += red[(w2 * REGS + r) * 32 + lane];
+    }
+  }
+}
+
+/* Completes the combines this CTA's arrivals finished (duty, filled by cta_merge). A first-level
+   duty sums its kFan (or fewer) pieces, stores the sum over the group's first piece and arrives at
+   the segment's counter; the CTA completing that counter (or a duty of a short segment) sums the
+   segment's pieces or first-level sums in order and writes the block once. Called by all threads
+   after a CTA barrier that follows cta_merge; ends with a barrier. */
 template <int MT, int NT>
-__device__ __forceinline__ void finish_segments(const StackTask& tk, int sub, int (*duty)[4], double* red) {
+__device__ __forceinline__ void finish_segments(const StackTask& tk, int sub, int (*duty)[6], double* red) {
   constexpr int REGS = MT * NT * 2;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5, g = lane >> 2, t = lane & 3;
+  __shared__ int s_go;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const int nsub = tk.nsub;
   for (int d = 0; d < 2; ++d) {
     if (0 == duty[d][0]) continue; /* uniform: shared memory read after a barrier */
-    const int j0 = duty[d][1], np = duty[d][2];
+    const int j0 = duty[d][1], np = duty[d][2], level = duty[d][4], i1 = duty[d][5];
     const unsigned key = (unsigned)duty[d][3];
-    __threadfence(); /* the other groups' pieces were published before their arrivals */
+    __threadfence(); /* the other CTAs published their pieces before their arrivals */
     double acc[REGS];
+    int count = np, stride = 1; /* what the final sum covers: pieces 0, stride, 2 * stride, ... */
+    if (1 == level) {
+      const int q1 = i1 * kFan, n1 = min(kFan, np - q1);
+      sum_pieces<REGS>(tk, sub, n1, [&](int i) { return piece_slot(j0, q1 + i); }, red, acc);
+      if (0 == warp) { /* the first-level sum replaces the group's first piece */
+        double* const dst = tk.pieces + ((size_t)piece_slot(j0, q1) * nsub + sub) * REGS * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
-    int q = warp;
-    for (; q + W < np; q += 2 * W) { /* two pieces in flight per step */
-      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q), s1 = 2 * (j0 + q + W);
-      const double* const p0 = tk.pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
-      const double* const p1 = tk.pieces + ((size_t)s1 * nsub + sub) * REGS * 32 + lane;
-      double v0[REGS], v1[REGS];
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) {
-        v0[r] = __ldcg(p0 + r * 32);
-        v1[r] = __ldcg(p1 + r * 32);
+        for (int r = 0; r < REGS; ++r) __stcg(dst + r * 32, acc[r]);
+        __threadfence();
+        __syncwarp();
+        int last = 0;
+        if (0 == lane) last = (atomicAdd(tk.arrive + (size_t)j0 * nsub + sub, 1) == (np + kFan - 1) / kFan - 1) ? 1 : 0;
+        if (0 == lane) s_go = last;
       }
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) acc[r] += v0[r];
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) acc[r] += v1[r];
+      __syncthreads();
+      const int go = s_go;
+      __syncthreads(); /* red and s_go may be reused */
+      if (!go) continue;
+      __threadfence();
+      count = (np + kFan - 1) / kFan;
+      stride = kFan;
     }
-    if (q < np) {
-      const int s0 = (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q);
-      const double* const p0 = tk.pieces + ((size_t)s0 * nsub + sub) * REGS * 32 + lane;
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) acc[r] += __ldcg(p0 + r * 32);
-    }
-    if (0 != warp) {
-#pragma unroll
-      for (int r = 0; r < REGS; ++r) red[((warp - 1) * REGS + r) * 32 + lane] = acc[r];
-    }
-    __syncthreads();
+    sum_pieces<REGS>(tk, sub, count, [&](int i) { return piece_slot(j0, i * stride); }, red, acc);
     if (0 == warp) {
-      for (int w2 = 0; w2 < W - 1; ++w2) {
-#pragma unroll
-        for (int r = 0; r < REGS; ++r) acc[r] += red[(w2 * REGS + r) * 32 + lane];
-      }
       Tile<MT, NT> tl;
       tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
       double tile[MT][NT][2];
@@ -477,7 +529,7 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
     }
   }
   __syncthreads();
-  __shared__ int duty[2][4];
+  __shared__ int duty[2][6];
   cta_merge<MT, NT>(tk, group, sub, seglist, meta, W,
     [&](int w, int slot) -> const double* { return sp + ((size_t)(w * 2 + slot) * REGS) * 32; }, duty);
   __syncthreads();
@@ -530,8 +582,10 @@ struct Staged {
                     : 4 * GQ + ((1 == QR) ? 4 * (s - GQ) + t : (s - GQ) + QR * t);
   }
   __host__ __device__ static constexpr int warp_bytes(int R) { return (R * STAGE > PIECES) ? R * STAGE : PIECES; }
+  /* + 256 bytes of slack: fragment reads of padding rows / columns may pass the last stage by up to
+     8 * MT - M_ (8 * NT - N_) doubles */
   __host__ __device__ static constexpr size_t smem_bytes(int W, int R) {
-    return (size_t)W * warp_bytes(R) + (size_t)W * R * sizeof(uint64_t) + (size_t)W * 4 * sizeof(int);
+    return (size_t)W * warp_bytes(R) + (size_t)W * R * sizeof(uint64_t) + (size_t)W * 4 * sizeof(int) + 256;
   }
 };
 
@@ -587,6 +641,9 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
   const int chunk = group * W + warp;
   Tile<MT, NT> tl;
   tl.init(0, 1, M_, N_, g);
+  /* per-lane fragment offsets (doubles): full k groups (stride Q), remainder steps (stride QR) */
+  const int lane_af = g + G::Q * M_ * t, lane_bf = g + G::Q * N_ * t;
+  const int lane_ar = g + G::QR * M_ * t, lane_br = g + G::QR * N_ * t;
   double acc[MT][NT][2], hacc[MT][NT][2];
 #pragma unroll
   for (int i = 0; i < MT; ++i)
@@ -661,14 +718,30 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
       const double* const sA = (const double*)(ring + st * G::STAGE) + (((uintptr_t)(A + ((unsigned)v - 1u)) >> 3) & 1u);
       const double* const sB =
         (const double*)(ring + st * G::STAGE + G::SA) + (((uintptr_t)(B + ((unsigned)(v >> 32) - 1u)) >> 3) & 1u);
+      /* fragments: lane (g, t) reads A(8i + g, kidx(ks, t)) and B(kidx(ks, t), 8j + g). Rows beyond
+         m and columns beyond n read whatever follows in shared memory (the stage, the next one, or
+         the slack after the last): they only reach C entries that are never written back. k indices
+         beyond k occur only in the remainder steps, where both fragments are zeroed. */
 #pragma unroll
       for (int ks = 0; ks < KS; ++ks) {
-        const int kk = G::kidx(ks, t);
         double fa[MT], fb[NT];
+        if (ks < G::GQ) { /* full groups: kidx = kc + Q*t, always inside the block */
+          constexpr int Q = G::Q;
+          const int kc = 4 * Q * (ks / Q) + ks % Q;
 #pragma unroll
-        for (int i = 0; i < MT; ++i) fa[i] = (kk < K_ && tl.rok[i]) ? sA[kk * M_ + 8 * i + g] : 0.0;
+          for (int i = 0; i < MT; ++i) fa[i] = sA[lane_af + kc * M_ + 8 * i];
 #pragma unroll
-        for (int j = 0; j < NT; ++j) fb[j] = (kk < K_ && tl.cok[j]) ? sB[kk * N_ + 8 * j + g] : 0.0;
+          for (int j = 0; j < NT; ++j) fb[j] = sB[lane_bf + kc * N_ + 8 * j];
+        }
+        else {
+          constexpr int QR = G::QR;
+          const int kc = 4 * G::GQ + ((1 == QR) ? 4 * (ks - G::GQ) : (ks - G::GQ));
+          const bool kin = kc + QR * t < K_;
+#pragma unroll
+          for (int i = 0; i < MT; ++i) fa[i] = kin ? sA[lane_ar + kc * M_ + 8 * i] : 0.0;
+#pragma unroll
+          for (int j = 0; j < NT; ++j) fb[j] = kin ? sB[lane_br + kc * N_ + 8 * j] : 0.0;
+        }
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
@@ -741,7 +814,7 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
     if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
     return;
   }
-  __shared__ int duty[2][4];
+  __shared__ int duty[2][6];
   cta_merge<MT, NT>(tk, group, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
     return (const double*)(smraw + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
   }, duty);
@@ -1012,8 +1085,8 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   off = align_up(off + sizeof(int) * ((size_t)pl->ngroups + 1), 256);
   pl->off_pieces = off;
   off = align_up(off + sizeof(double) * (size_t)2 * pl->ngroups * pl->nsub * (mt * nt * 2) * 32, 256);
-  pl->off_arrive = off;
-  off = align_up(off + sizeof(int) * (size_t)pl->ngroups * pl->nsub, 256);
+  pl->off_arrive = off; /* segment counters [ngroups][nsub], then first-level counters [2 ngroups][nsub] */
+  off = align_up(off + sizeof(int) * (size_t)3 * pl->ngroups * pl->nsub, 256);
   pl->off_sort = off;
   off = align_up(off + xs_stack_sort_scratch_bytes(S), 256);
   pl->total = off;
@@ -1503,7 +1576,7 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   int* const arrive = (int*)(base + pl.off_arrive);
   void* prof = xs_profile_begin(s);
   const int r = xs_stack_group_ex(dev_stack, S, format, (unsigned)(m * n), keys_in, vals_in, keys_tmp, vals_tmp, keys_out,
-    vals_out, seglist, arrive, pl.ngroups * pl.nsub, sort_scratch, s);
+    vals_out, seglist, arrive, 3 * pl.ngroups * pl.nsub, sort_scratch, s);
   if (0 != r) return r;
   xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
   StackTask tk = {};

@@ -428,47 +428,51 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
 
 /* ------------------------------------------------------------------ one-cluster grouping (small stacks) */
 
-/* Largest cluster the one-cluster grouping uses (16: non-portable size, one GPC) and the most entries
-   it takes (16 CTAs x 2048, or 8 CTAs x 4096 where clusters of 16 are not available). */
+/* One-cluster grouping: 16 CTAs of 512 threads, 4 entries per thread (32768 entries at most). */
 constexpr int kClusterMax = 16;
-constexpr int kClusterEntries = kClusterMax * kSortThreads * 8;
+constexpr int kClThreads = 512;
+constexpr int kClWarps = kClThreads / 32;
+constexpr int kClE = 4;
+constexpr int kClusterEntries = kClusterMax * kClThreads * kClE;
+/* dynamic shared memory: per-warp digit counters [kClWarps][kRadix] (u16), then the digit totals of
+   every CTA of the cluster [kClusterMax][kRadix] (int) */
+constexpr size_t kClSmem = sizeof(unsigned short) * kClWarps * kRadix + sizeof(int) * kClusterMax * kRadix;
 
-/* Bucket floor(x / d) from a double reciprocal with a one-step correction (exact for x < 2^32). */
-__device__ __forceinline__ unsigned bucket_floor(unsigned x, unsigned d, double inv_d) {
-  unsigned q = (unsigned)((double)x * inv_d);
-  const unsigned long long p = (unsigned long long)q * d;
-  if (p > x) --q;
-  else if (p + d <= x) ++q;
+/* floor(x / d) for d >= 1 from m = floor(2^32 / d) (m = 0 for d = 1): the high product is q or
+   q - 1, one correction step fixes it. */
+__device__ __forceinline__ unsigned div_floor(unsigned x, unsigned d, unsigned m) {
+  if (1u >= d) return x;
+  unsigned q = __umulhi(x, m);
+  if ((unsigned long long)(q + 1u) * d <= x) ++q;
   return q;
 }
 
-/* Grouping of one stack of at most kClusterEntries entries by ONE thread-block cluster: the same
-   stable LSD counting sort as xs_stack_group_kernel (same tiles, digits and ranks, hence the same
-   output), with the cluster's CTAs exchanging statistics and counts by pushing them into each
-   other's shared memory between cluster barriers: no grid-wide barrier, global histogram table or
-   atomic statistics, and no memset (CTA 0 clears the error word and the segment list). Bucket ids:
-   with blk > 0 (the C block size: blocks of one stack do not overlap, so distinct blocks lie at least
-   blk apart) id = (c - cmin) / blk, which needs only the minimum and maximum; with blk == 0 the gcd
-   of the offset differences divides them exactly, as in xs_stack_group_kernel. Per pass, each warp
-   counts its entries per digit (match masks, one count per distinct digit), the per-digit totals of
-   the CTA follow from the per-warp counts, the digits' owner CTAs (digit d: CTA d / DR) turn the
-   counts of all CTAs into write positions and push them back, and every warp places its entries in
-   stack order. Cluster barriers are hardware barriers of co-scheduled CTAs and cannot hang. */
+/* Grouping of one stack of at most kClusterEntries entries by ONE thread-block cluster: a stable LSD
+   counting sort over the bucket ids of the c offsets, with the same per-digit order as
+   xs_stack_group_kernel (stack order within a digit, hence the same output). Bucket ids: with blk > 0
+   (the C block size: the blocks of one stack do not overlap, so distinct blocks lie at least blk
+   apart) id = (c - cmin) / blk, which needs only the minimum and maximum of the offsets; with
+   blk == 0 the gcd of the offset differences divides them exactly. The CTAs exchange data only by
+   pushing it into each other's shared memory, each push followed by a cluster barrier: their
+   statistics, then per pass their digit totals, from which every CTA derives its write positions
+   locally (totals over the cluster, exclusive scan over the digits, counts of the CTAs before it).
+   Within a CTA, each warp counts its entries per digit from match masks (one count per distinct
+   digit and entry round) and places them in stack order. No grid barrier, global table, atomic or
+   memset (CTA 0 clears the error word and the segment list); cluster barriers are hardware
+   barriers of co-scheduled CTAs and cannot hang. */
 template <int E>
-__global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(const int* __restrict__ stack, int S, int format,
+__global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(const int* __restrict__ stack, int S, int format,
   unsigned blk, unsigned* __restrict__ k0, unsigned long long* __restrict__ v0, unsigned* __restrict__ k1,
   unsigned long long* __restrict__ v1, unsigned* __restrict__ kout, unsigned long long* __restrict__ vout,
   int* __restrict__ seglist, int* __restrict__ zero, int nzero, SortCtl* ctl) {
   namespace cg = cooperative_groups;
-  extern __shared__ __align__(16) unsigned short s_wc_raw[]; /* [kSortWarps][kRadix] (dynamic: static memory is full) */
-  unsigned short (*const s_wc)[kRadix] = reinterpret_cast<unsigned short (*)[kRadix]>(s_wc_raw);
-  __shared__ int s_hist[kRadix]; /* this CTA's digit totals */
-  __shared__ int s_gath[kRadix]; /* [q][dl]: CTA q's count of owned digit dl, pushed by q */
-  __shared__ int s_base[kRadix]; /* digit write positions of this CTA, pushed by the digits' owners */
-  __shared__ int s_wsum[kSortWarps];
-  __shared__ unsigned s_red[3][kSortWarps];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  unsigned short (*const s_wc)[kRadix] = reinterpret_cast<unsigned short (*)[kRadix]>(s_dyn);
+  int (*const s_all)[kRadix] = reinterpret_cast<int (*)[kRadix]>(s_dyn + sizeof(unsigned short) * kClWarps * kRadix);
+  __shared__ int s_base[kRadix]; /* digit write positions of this CTA */
+  __shared__ int s_wsum[kClWarps];
+  __shared__ unsigned s_red[3][kClWarps];
   __shared__ unsigned s_stat[kClusterMax][3]; /* cmin, cmax, gcd of every CTA, pushed by each */
-  __shared__ int s_slice[kClusterMax];          /* digit-slice totals of every owner, pushed by each */
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
   asm volatile("griddepcontrol.launch_dependents;" :::);
@@ -476,7 +480,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
      now, wait before the first push (the stack loads overlap the barrier) */
   asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
   const int pstride = (0 != format) ? 6 : 3, pbase = (0 != format) ? 3 : 0, pone = (0 != format) ? 1 : 0;
-  const int T = kSortThreads * E;
+  const int T = kClThreads * E;
   const int t0 = min(S, rank * T), t1 = min(S, t0 + T);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w0 = min(t1, t0 + warp * 32 * E), w1 = min(t1, w0 + 32 * E);
@@ -486,7 +490,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
     ctl->err = 0u;
     if (nullptr != seglist) seglist[0] = 0;
   }
-  for (int i = rank * kSortThreads + (int)threadIdx.x; i < nzero; i += ncta * kSortThreads) zero[i] = 0;
+  for (int i = rank * kClThreads + (int)threadIdx.x; i < nzero; i += ncta * kClThreads) zero[i] = 0;
   { /* load + statistics */
     unsigned lo = 0xFFFFFFFFu, hi = 0u, gg = 0u;
 #pragma unroll
@@ -521,12 +525,12 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
     }
     __syncthreads();
     if (0 == warp) {
-      lo = (lane < kSortWarps) ? s_red[0][lane] : 0xFFFFFFFFu;
-      hi = (lane < kSortWarps) ? s_red[1][lane] : 0u;
+      lo = (lane < kClWarps) ? s_red[0][lane] : 0xFFFFFFFFu;
+      hi = (lane < kClWarps) ? s_red[1][lane] : 0u;
       lo = __reduce_min_sync(0xffffffffu, lo);
       hi = __reduce_max_sync(0xffffffffu, hi);
       if (0 == lane && 0 == blk) {
-        for (int w = 1; w < kSortWarps; ++w) gg = gcd_acc(gg, s_red[2][w]);
+        for (int w = 1; w < kClWarps; ++w) gg = gcd_acc(gg, s_red[2][w]);
       }
       gg = __shfl_sync(0xffffffffu, gg, 0);
     }
@@ -545,8 +549,8 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
     cmax = max(cmax, s_stat[q][1]);
     if (0 == blk) g = gcd_acc(g, s_stat[q][2]);
   }
-  const unsigned nb = (0 == g) ? 1u : (cmax - cmin) / g + 1u;
-  const double inv_g = (0 == g) ? 0.0 : 1.0 / (double)g;
+  const unsigned gm = (1u < g) ? (unsigned)((1ull << 32) / g) : 0u;
+  const unsigned nb = (0 == g) ? 1u : div_floor(cmax - cmin, g, gm) + 1u;
   int bits = 0;
   while (bits < 32 && (nb - 1u) >> bits) ++bits;
   const int passes = (bits + kRadixBits - 1) / kRadixBits;
@@ -561,6 +565,9 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
     }
   }
   const int rb = (0 == passes) ? 0 : (bits + passes - 1) / passes, R = 1 << rb;
+  unsigned id[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) id[r] = (0 == g) ? 0u : div_floor(key[r] - cmin, g, gm);
   for (int pass = 0; pass < passes; ++pass) {
     const int shift = pass * rb;
     const bool last = (pass + 1 == passes);
@@ -568,83 +575,65 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
     unsigned long long* const vdst = last ? vout : ((0 == (pass & 1)) ? v1 : v0);
     int dig[E];
 #pragma unroll
-    for (int r = 0; r < E; ++r) {
-      dig[r] = (w0 + lane + 32 * r < w1) ? (int)((bucket_floor(key[r] - cmin, g, inv_g) >> shift) & (R - 1)) : kRadix;
+    for (int r = 0; r < E; ++r) dig[r] = (w0 + lane + 32 * r < w1) ? (int)((id[r] >> shift) & (R - 1)) : kRadix;
+    /* (a) per-warp digit counts: the leader of each group of equal digits adds the group's size */
+    if (R >= 8) {
+      for (int j = threadIdx.x; j < kClWarps * (R / 8); j += kClThreads) { /* 8 counters per 16-byte store */
+        reinterpret_cast<uint4*>(&s_wc[j / (R / 8)][0])[j % (R / 8)] = make_uint4(0u, 0u, 0u, 0u);
+      }
     }
-    /* (a) per-warp digit counts (the leader of each group of equal digits adds the group's size),
-       then per digit: exclusive prefix over the warps in place, CTA total */
-    for (int j = threadIdx.x; j < kSortWarps * R / 8; j += blockDim.x) { /* 8 counters per 16-byte store */
-      const int w = j / (R / 8), d8 = j - w * (R / 8);
-      if (R >= 8) reinterpret_cast<uint4*>(&s_wc[w][0])[d8] = make_uint4(0u, 0u, 0u, 0u);
-    }
-    if (R < 8 && (int)threadIdx.x < kSortWarps * R) s_wc[threadIdx.x / R][threadIdx.x % R] = 0;
+    else if ((int)threadIdx.x < kClWarps * R) s_wc[threadIdx.x / R][threadIdx.x % R] = 0;
     __syncthreads();
     unsigned peers[E];
 #pragma unroll
+    for (int r = 0; r < E; ++r) peers[r] = __match_any_sync(0xffffffffu, dig[r]);
+#pragma unroll
     for (int r = 0; r < E; ++r) {
-      peers[r] = __match_any_sync(0xffffffffu, dig[r]);
       if (kRadix != dig[r] && 0 == __popc(peers[r] & ((1u << lane) - 1u))) {
         s_wc[warp][dig[r]] += (unsigned short)__popc(peers[r]);
       }
       __syncwarp();
     }
     __syncthreads();
-    for (int dd = threadIdx.x; dd < R; dd += blockDim.x) {
+    /* (b) per digit: exclusive prefix over the warps in place; the CTA total goes to every CTA */
+    for (int d = threadIdx.x; d < R; d += kClThreads) {
       int run = 0;
 #pragma unroll
-      for (int w2 = 0; w2 < kSortWarps; ++w2) {
-        const int c = s_wc[w2][dd];
-        s_wc[w2][dd] = (unsigned short)run;
+      for (int w2 = 0; w2 < kClWarps; ++w2) {
+        const int c = s_wc[w2][d];
+        s_wc[w2][d] = (unsigned short)run;
         run += c;
       }
-      s_hist[dd] = run;
-    }
-    __syncthreads();
-    /* (b) digit bases. Digits are owned in slices of DR by the CTAs (digit d by CTA d / DR). Every
-       exchange is a push into another CTA's shared memory followed by a cluster barrier: counts to
-       the owners, slice totals to all, then each (digit, CTA) base to that CTA. */
-    const int DR = (R + ncta - 1) / ncta;
-    for (int d = threadIdx.x; d < R; d += blockDim.x) {
-      const int q = d / DR;
-      *cluster.map_shared_rank(&s_gath[rank * DR + (d - q * DR)], q) = s_hist[d];
+      for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(&s_all[rank][d], q) = run;
     }
     cluster.sync();
-    constexpr int PER = kRadix / kSortThreads;
-    const int per = (DR + kSortThreads - 1) / kSortThreads;
-    int tot[PER];
-#pragma unroll
-    for (int j = 0; j < PER; ++j) { /* owned digit dl: prefix over the CTAs in place, total */
-      const int dl = threadIdx.x * per + j;
-      int run = 0;
-      if (j < per && dl < DR && rank * DR + dl < R) {
-        for (int q = 0; q < ncta; ++q) {
-          const int x = s_gath[q * DR + dl];
-          s_gath[q * DR + dl] = run;
-          run += x;
-        }
-      }
-      tot[j] = run;
-    }
-    int slice = 0;
-#pragma unroll
-    for (int j = 0; j < PER; ++j) slice += tot[j];
-    block_exscan<PER>(tot, s_wsum);
-    if (kSortThreads - 1 == (int)threadIdx.x) { /* the last thread's exclusive start + its own sum */
-      for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(&s_slice[rank], q) = tot[0] + slice;
-    }
-    cluster.sync();
-    int slice_off = 0;
-    for (int q = 0; q < rank; ++q) slice_off += s_slice[q];
+    /* (c) write positions: exclusive scan of the cluster totals over the digits plus the counts of
+       the CTAs before this one. Thread i owns digits [i*per, (i+1)*per). */
+    constexpr int PER = kRadix / kClThreads;
+    const int per = (R + kClThreads - 1) / kClThreads;
+    int tot[PER], pre[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-      const int dl = threadIdx.x * per + j;
-      const int d = rank * DR + dl;
-      if (j < per && dl < DR && d < R) {
-        for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(&s_base[d], q) = slice_off + tot[j] + s_gath[q * DR + dl];
+      const int d = threadIdx.x * per + j;
+      int x = 0, p = 0;
+      if (j < per && d < R) {
+        for (int q = 0; q < ncta; ++q) {
+          const int c = s_all[q][d];
+          x += c;
+          p += (q < rank) ? c : 0;
+        }
       }
+      tot[j] = x;
+      pre[j] = p;
     }
-    cluster.sync();
-    /* (c) stable scatter in stack order: CTA base + warp offset + rank within the warp */
+    block_exscan<PER>(tot, s_wsum);
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int d = threadIdx.x * per + j;
+      if (j < per && d < R) s_base[d] = tot[j] + pre[j];
+    }
+    __syncthreads();
+    /* (d) stable placement in stack order: CTA base + warp offset + rank within the warp */
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const int rank_w = __popc(peers[r] & ((1u << lane) - 1u));
@@ -657,14 +646,15 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_cluster_kernel(co
       if (kRadix != dig[r] && 0 == rank_w) s_wc[warp][dig[r]] += (unsigned short)__popc(peers[r]);
       __syncwarp();
     }
-    if (!last) {
-      cluster.sync(); /* this pass's output is visible to the whole cluster */
+    if (!last) { /* this pass's output is visible to the whole cluster, and s_all may be overwritten */
+      cluster.sync();
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const int i = w0 + lane + 32 * r;
         if (i < w1) {
           key[r] = __ldcg(kdst + i);
           val[r] = __ldcg(vdst + i);
+          id[r] = (0 == g) ? 0u : div_floor(key[r] - cmin, g, gm);
         }
       }
     }
@@ -730,19 +720,18 @@ int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long*
     args, 0, s);
 }
 
-/* Launches the one-cluster grouping with ncta CTAs (a power of two <= kClusterMax) of E entries per
-   thread. Returns cudaErrorNotSupported, launching nothing, when the device cannot run a cluster of
-   that size. */
+/* Launches the one-cluster grouping with ncta CTAs (a power of two <= kClusterMax). Returns
+   cudaErrorNotSupported, launching nothing, when the device cannot run a cluster of that size. */
 int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, SortCtl* ctl, int ncta,
-  int E, cudaStream_t s) {
-  static int ok[2][kClusterMax + 1]; /* per E and cluster size: 0 unknown, 1 supported, -1 not */
-  auto kernel = (16 == E) ? xs_stack_group_cluster_kernel<16> : xs_stack_group_cluster_kernel<8>;
-  int* const okp = &ok[(16 == E) ? 1 : 0][ncta];
-  const size_t smem = sizeof(unsigned short) * kSortWarps * kRadix;
+  cudaStream_t s) {
+  static int ok[kClusterMax + 1]; /* per cluster size: 0 unknown, 1 supported, -1 not */
+  auto kernel = xs_stack_group_cluster_kernel<kClE>;
+  int* const okp = &ok[ncta];
+  const size_t smem = kClSmem;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)ncta);
-  cfg.blockDim = dim3(kSortThreads);
+  cfg.blockDim = dim3(kClThreads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -812,15 +801,11 @@ int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long
 int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
   void* stream) {
-  if (0 < S && S <= kClusterEntries) { /* one cluster: tiles of 2048 entries, else half as many of 4096 */
+  if (0 < S && S <= kClusterEntries) { /* one cluster of up to 16 CTAs */
     int ncta = 1;
-    while (ncta * kSortThreads * 8 < S) ncta <<= 1;
-    int r = cluster_group_launch(dev_stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero,
-      (SortCtl*)sort_scratch, ncta, 8, (cudaStream_t)stream);
-    if (cudaErrorNotSupported == r && 1 < ncta) {
-      r = cluster_group_launch(dev_stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero,
-        (SortCtl*)sort_scratch, ncta / 2, 16, (cudaStream_t)stream);
-    }
+    while (ncta * kClThreads * kClE < S) ncta <<= 1;
+    const int r = cluster_group_launch(dev_stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero,
+      (SortCtl*)sort_scratch, ncta, (cudaStream_t)stream);
     if (cudaErrorNotSupported != r) return r; /* else: the cooperative kernel below */
   }
   xs_sort_batch_t d;
