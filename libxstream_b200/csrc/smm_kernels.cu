@@ -572,8 +572,13 @@ struct Staged {
      start Q*M_*8 bytes apart; when Q*M_ mod 16 is 4 or 12 (in doubles) the four 4-lane groups of a
      half-warp land on four disjoint sets of banks. Full groups of 4*Q indices use stride Q; the
      remainder uses Q too when that costs no extra step, else stride 1. */
-  static constexpr bool spread(int q) { return ((q * M_) % 16 == 4 || (q * M_) % 16 == 12) && ((q * N_) % 16 == 4 || (q * N_) % 16 == 12); }
-  static constexpr int Q = spread(1) ? 1 : (spread(2) ? 2 : (spread(4) ? 4 : 1));
+  static constexpr bool spread_one(int q, int ld) { return (q * ld) % 16 == 4 || (q * ld) % 16 == 12; }
+  static constexpr bool spread(int q) { return spread_one(q, M_) && spread_one(q, N_); }
+  /* a stride that spreads both operands, else one that spreads A (the larger share of the loads
+     when m >= n), else B */
+  static constexpr int Q = spread(1) ? 1 : spread(2) ? 2 : spread(4) ? 4
+                         : spread_one(1, M_) ? 1 : spread_one(2, M_) ? 2 : spread_one(4, M_) ? 4
+                         : spread_one(1, N_) ? 1 : spread_one(2, N_) ? 2 : spread_one(4, N_) ? 4 : 1;
   static constexpr int GQ = (K_ / (4 * Q)) * Q; /* steps in full groups */
   static constexpr int RS = KS - GQ;             /* remainder steps */
   static constexpr int QR = (RS == Q) ? Q : 1;
@@ -1173,17 +1178,21 @@ struct SpecEntry {
 };
 #define XS_SPEC(S, MT, KP) {S, S, S, MT, MT, KP, &launch_dmma<S, S, S, MT, MT, KP>}
 #define XS_STAGED(S, R) {S, S, S, (S + 7) / 8, (S + 7) / 8, 0, &launch_staged<S, S, S, R>}
+#define XS_STAGED3(M, N, K, R) {M, N, K, (M + 7) / 8, (N + 7) / 8, 0, &launch_staged<M, N, K, R>}
 static const SpecEntry spec_table[] = {
   XS_SPEC(4, 1, 1), XS_SPEC(5, 1, 2), XS_SPEC(8, 1, 2), XS_SPEC(9, 2, 3), XS_SPEC(16, 2, 2), XS_SPEC(16, 2, 4),
   XS_SPEC(32, 4, 2), XS_SPEC(32, 4, 4), XS_SPEC(45, 3, 2), XS_SPEC(45, 3, 4), XS_SPEC(64, 4, 2), XS_SPEC(64, 4, 4),
 };
 
 /* Shapes with a staged kernel: it runs whenever the warp tile covers the whole C block (any kp),
-   unless the runtime-shape kernel is forced (generic). For block sizes that are multiples of 8 the
-   column stride puts every column on the same banks and staging does not pay; those keep the
-   register kernel. */
+   unless the runtime-shape kernel is forced (generic). Each was measured against the register
+   kernel on stacks of 30000 entries; 5^3 (no gain) and 32^3 (slower: a 256-byte column stride puts
+   every fragment column on the same banks) keep the register kernel, like every shape not listed. */
 static const SpecEntry staged_table[] = {
   XS_STAGED(13, 2), XS_STAGED(22, 2), XS_STAGED(23, 2), XS_STAGED(26, 2),
+  XS_STAGED3(23, 22, 13, 2), XS_STAGED3(22, 22, 23, 2), XS_STAGED3(32, 9, 9, 2), XS_STAGED3(13, 4, 16, 2),
+  XS_STAGED(4, 2), XS_STAGED(8, 2), XS_STAGED(9, 2), XS_STAGED(16, 2), XS_STAGED3(16, 26, 5, 2), XS_STAGED3(26, 23, 26, 2),
+  XS_STAGED3(22, 32, 32, 2),
 };
 
 launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {

@@ -12,7 +12,9 @@ from test_smm_gpu import TOL, oracle_c, run_device
 
 pytestmark = pytest.mark.gpu
 
-STAGED = [13, 16, 22, 23, 26, 32]  # square shapes with a staged kernel
+STAGED = [4, 8, 9, 13, 16, 22, 23, 26, 32]  # square shapes (32: the register kernel runs)
+STAGED3 = [(23, 22, 13), (22, 22, 23), (32, 9, 9), (13, 4, 16), (16, 26, 5), (26, 23, 26),
+           (22, 32, 32)]  # non-square shapes with a staged kernel
 
 
 def _run_with(A, stream, case, chunk, kp, wpb=4, c0=None):
@@ -69,3 +71,14 @@ def test_staged_single_entry(acc):
     A, stream = acc
     case = W.stack_case(16, 16, 16, 1, 3, 3, 1, seed=6)
     assert oracle.block_relerr(_run_with(A, stream, case, 0, 0), oracle_c(case), 256) <= TOL
+
+
+@pytest.mark.parametrize("shape", STAGED3, ids=[f"{m}x{n}x{k}" for m, n, k in STAGED3])
+@pytest.mark.parametrize("chunk", [0, 1, 40])
+def test_staged_nonsquare_parity(acc, shape, chunk):
+    A, stream = acc
+    m, n, k = shape
+    case = W.stack_case(m, n, k, 3000, 211, 197, 41, seed=m * 1000 + n * 10 + k + chunk)
+    c0 = W.rng(k).uniform(-1, 1, size=case.nc * m * n)
+    got = _run_with(A, stream, case, chunk, 0, c0=c0)
+    assert oracle.block_relerr(got, oracle_c(case, c0=c0), m * n) <= TOL
