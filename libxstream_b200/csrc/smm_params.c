@@ -128,6 +128,20 @@ void xs_params_lookup_ex(int type, int m, int n, int k, int stack_size, xs_smm_p
       xs_sanitize(out);
       if (NULL != source) *source = (conf >= xs_mlp_minconf()) ? XS_PARAMS_PREDICTED : XS_PARAMS_LOWCONF;
     }
+    { /* a staged kernel compiled for the shape (listed with kp = 0) beat the register kernel's
+         configurations where it was measured: its whole-block tile replaces heuristic and predicted
+         tiles (tuned records stay as recorded) */
+      int triples[3 * 8], i;
+      const int nspec = xs_smm_f64_specialized(m, n, k, triples, 8);
+      for (i = 0; i < nspec && i < 8; ++i) {
+        if (0 == triples[3 * i + 2]) {
+          out->mt = triples[3 * i];
+          out->nt = triples[3 * i + 1];
+          out->kp = 0;
+          break;
+        }
+      }
+    }
   }
 }
 

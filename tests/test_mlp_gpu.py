@@ -93,7 +93,10 @@ def test_install_drives_parameter_lookup(acc):
             assert P.config_index(out[0], out[1], out[2]) == int(rc[0])
             p6 = (ctypes.c_int * 6)()
             lib.libxstream_b200_get_params(m, n, k, S, p6)
-            assert (p6[1], p6[2], p6[3]) == (out[0], out[1], out[2])
+            if (m, n, k) == (23, 23, 23):  # a staged kernel exists: its whole-block tile is used instead
+                assert (p6[1], p6[2], p6[3]) == (3, 3, 0)
+            else:
+                assert (p6[1], p6[2], p6[3]) == (out[0], out[1], out[2])
     finally:
         assert lib.libxstream_b200_mlp_install(None, 0) == 0
     out = (ctypes.c_int * 3)()
