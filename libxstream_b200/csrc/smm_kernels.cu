@@ -1054,7 +1054,7 @@ launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm);
    sized so that the grid is one full wave of resident CTAs: L = ceil(S * nsub / (resident * W)). */
 int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl) {
   const int mt = prm->mt, nt = prm->nt;
-  if (mt < 1 || mt > 4 || nt < 1 || nt > 4) return -1;
+  if (mt < 1 || mt > 8 || nt < 1 || nt > 8) return -1; /* tiles beyond 4 fragments: staged kernels only */
   pl->no_combine = 0;
   pl->nsub_m = ((m + 7) / 8 + mt - 1) / mt;
   pl->nsub_n = ((n + 7) / 8 + nt - 1) / nt;
@@ -1192,8 +1192,12 @@ static const SpecEntry staged_table[] = {
   XS_STAGED(13, 2), XS_STAGED(22, 2), XS_STAGED(23, 2), XS_STAGED(26, 2),
   XS_STAGED3(23, 22, 13, 2), XS_STAGED3(22, 22, 23, 2), XS_STAGED3(32, 9, 9, 2), XS_STAGED3(13, 4, 16, 2),
   XS_STAGED(4, 2), XS_STAGED(8, 2), XS_STAGED(9, 2), XS_STAGED(16, 2), XS_STAGED3(16, 26, 5, 2), XS_STAGED3(26, 23, 26, 2),
-  XS_STAGED3(22, 32, 32, 2),
+  XS_STAGED3(22, 32, 32, 2), XS_STAGED3(16, 64, 9, 2),
 };
+
+cudaError_t launch_unsupported(const SmmPlan&, const StackTask&, int*, const unsigned*, cudaStream_t, int*) {
+  return cudaErrorInvalidValue;
+}
 
 launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
   if (0 == prm->generic) {
@@ -1204,6 +1208,7 @@ launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
       if (e.m == m && e.n == n && e.k == k && e.mt == prm->mt && e.nt == prm->nt && e.kp == prm->kp) return e.fn;
     }
   }
+  if (prm->mt > 4 || prm->nt > 4) return &launch_unsupported; /* no register kernel for such tiles */
   return launch_table[prm->mt - 1][prm->nt - 1][(4 == prm->kp) ? 1 : 0];
 }
 
@@ -1296,6 +1301,8 @@ struct BatchPlan {
   size_t off_part[kMaxBatchTasks], pieces_off[kMaxBatchTasks];
   int order[kMaxBatchTasks]; /* parts by descending item cost */
   size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces, off_sort;
+  size_t off_arrive, narrive;             /* arrival counters of the solo parts (in-kernel combine) */
+  size_t arrive_off[kMaxBatchTasks];
   size_t total;
 };
 
@@ -1344,7 +1351,20 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     const long resident = (long)occ * xs_sm_count();
     solo_L[q] = (int)(((long)p.S * nsub + resident * kBatchW - 1) / (resident * kBatchW));
     p.solo = (solo_L[q] >= kSoloMinL) ? 1 : 0;
-    if (!p.solo) total[batch_group(p.mt, p.nt)] += (double)p.S * nsub * (p.mt * p.nt * ((d.k + 3) / 4) + 8);
+    if (!p.solo && (p.mt > 4 || p.nt > 4)) { /* the persistent kernels take tiles of up to 4 x 4 fragments */
+      p.mt = p.prm.mt = min(p.mt, 4);
+      p.nt = p.prm.nt = min(p.nt, 4);
+      if (0 == p.prm.kp) p.prm.kp = 2;
+    }
+    if (!p.solo) {
+      const int nsub2 = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
+      total[batch_group(p.mt, p.nt)] += (double)p.S * nsub2 * (p.mt * p.nt * ((d.k + 3) / 4) + 8);
+    }
+  }
+  bp->X = 1; /* the batch combine serves the shared-queue parts only: solo parts combine in their kernel */
+  for (int q = 0; q < bp->nparts; ++q) {
+    if (bp->part[q].solo) continue;
+    bp->X = max(bp->X, max(bp->part[q].mt, bp->part[q].nt));
   }
   double target[2];
   for (int grp = 0; grp < 2; ++grp) {
@@ -1352,7 +1372,7 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     if (cudaSuccess != batch_occupancy(grp, &occ) || occ < 1) occ = 1;
     target[grp] = total[grp] / ((double)occ * xs_sm_count() * 2.0);
   }
-  size_t off = 0, poff = 0;
+  size_t off = 0, poff = 0, narrive = 0;
   bp->ngroups_total = 0;
   bp->nitems = 0;
   for (int q = 0; q < bp->nparts; ++q) {
@@ -1372,6 +1392,8 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     off += (size_t)p.S;
     bp->pieces_off[q] = poff;
     poff += (size_t)2 * bp->ngroups[q] * bp->nsub[q] * (p.mt * p.nt * 2) * 32;
+    bp->arrive_off[q] = narrive;
+    if (p.solo) narrive += (size_t)3 * bp->ngroups[q] * bp->nsub[q];
     bp->ngroups_total += bp->ngroups[q];
     if (!p.solo) bp->nitems += bp->ngroups[q] * bp->nsub[q];
     bp->order[q] = q;
@@ -1404,6 +1426,9 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
   o = align_up(o + sizeof(int) * ((size_t)bp->ngroups_total + 1), 256);
   bp->off_pieces = o;
   o = align_up(o + sizeof(double) * poff, 256);
+  bp->off_arrive = o;
+  bp->narrive = narrive;
+  o = align_up(o + sizeof(int) * narrive, 256);
   bp->off_sort = o;
   o = align_up(o + xs_sort_ctl_bytes() + sizeof(int) * ((size_t)xs_sort_launch_tiles() + XS_MAX_BATCH) * 2048, 256);
   bp->total = o;
@@ -1633,12 +1658,16 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
   int* const seglist = (int*)(base + bp.off_seglist);
   double* const pieces = (double*)(base + bp.off_pieces);
   void* const sort_scratch = base + bp.off_sort;
-  /* grouping: one control block for the call, then as few grouping launches as the tiles need */
+  int* const arrive = (int*)(base + bp.off_arrive);
+  /* grouping: one control block for the call, then as few grouping launches as the tiles need; the
+     first one also zeroes the solo parts' arrival counters */
   int r = xs_sort_clear_ctl(sort_scratch, bp.nparts, s);
   if (0 != r) return r;
   void* prof = xs_profile_begin(s);
   xs_sort_batch_t sb;
   memset(&sb, 0, sizeof(sb));
+  sb.zero = (0 < bp.narrive) ? arrive : nullptr;
+  sb.nzero = (int)bp.narrive;
   int tiles = 0;
   const int launch_tiles = xs_sort_launch_tiles(), tile_entries = xs_sort_tile_entries(1);
   for (int q = 0; q <= bp.nparts; ++q) {
@@ -1647,6 +1676,8 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
       if (0 < sb.nstacks) {
         r = xs_stack_group_batch(&sb, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, s);
         if (0 != r) return r;
+        sb.zero = nullptr;
+        sb.nzero = 0;
       }
       sb.nstacks = 0;
       tiles = 0;
@@ -1704,6 +1735,7 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
       pl.nsub_n = tk.nsub_n;
       pl.nsub = tk.nsub;
       pl.no_combine = 1;
+      tk.arrive = arrive + bp.arrive_off[q]; /* its CTA-crossing segments are combined in its kernel */
       r = (int)find_launcher(d.m, d.n, d.k, &p.prm)(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
       if (0 != r) return r;
       continue;

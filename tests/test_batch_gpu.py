@@ -160,3 +160,26 @@ def test_batch_rejects_unsuitable_stacks(acc):
     assert not np.any(d.result(stream))  # nothing was done
     assert A.lib().libxstream_b200_process_batch(None, 0, 80, stream.handle) == 0
     d.free()
+
+
+def test_batch_solo_parts_combine_in_kernel(acc):
+    """Large parts run alone and combine their CTA-crossing segments inside their own kernel (staged
+    kernels, one with a 2 x 8-fragment tile); small parts of the same shapes share the persistent
+    kernels (tiles clamped to 4 x 4) and the batch combine. Parity and bitwise reproducibility."""
+    A, stream = acc
+    cases = [W.stack_case(16, 64, 9, 120000, 2000, 2000, 500, seed=701),
+             W.stack_case(16, 64, 9, 900, 100, 100, 30, seed=702),
+             W.stack_case(23, 23, 23, 90000, 2000, 2000, 400, seed=703),
+             W.stack_case(23, 23, 23, 700, 50, 50, 20, seed=704),
+             W.stack_case(45, 45, 45, 2000, 100, 100, 40, seed=705)]
+    devs = [DevCase(A, stream, c, c0=W.rng(i).uniform(-1, 1, size=c.nc * c.m * c.n)) for i, c in enumerate(cases)]
+    assert run_batch(A, stream, devs) == 0
+    first = [d.result(stream) for d in devs]
+    for d, got in zip(devs, first):
+        assert oracle.block_relerr(got, d.reference(), d.case.m * d.case.n) <= TOL, (d.case.m, d.case.n, d.case.k)
+    for d in devs:  # same inputs again from the same C: bitwise equal results
+        d.c.upload(d.c0, stream)
+    assert run_batch(A, stream, devs) == 0
+    for d, got in zip(devs, first):
+        assert np.array_equal(d.result(stream), got)
+        d.free()

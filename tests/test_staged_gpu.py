@@ -82,3 +82,16 @@ def test_staged_nonsquare_parity(acc, shape, chunk):
     c0 = W.rng(k).uniform(-1, 1, size=case.nc * m * n)
     got = _run_with(A, stream, case, chunk, 0, c0=c0)
     assert oracle.block_relerr(got, oracle_c(case, c0=c0), m * n) <= TOL
+
+
+def test_staged_wide_tile_parity(acc):
+    """16x64x9: the staged kernel with a warp tile of 2 x 8 fragments (wider than the register kernels
+    take), chosen by the untuned parameter lookup; C accumulates onto existing content."""
+    A, stream = acc
+    A.lib().libxstream_b200_clear_params()
+    p = A.get_params(16, 64, 9, 30000)
+    assert (p["mt"], p["nt"], p["kp"]) == (2, 8, 0)
+    case = W.stack_case(16, 64, 9, 30000, 800, 800, 300, seed=1664)
+    c0 = W.rng(9).uniform(-1, 1, size=case.nc * 16 * 64)
+    got = run_device(A, stream, case, c0=c0)
+    assert oracle.block_relerr(got, oracle_c(case, c0=c0), 16 * 64) <= TOL
