@@ -58,6 +58,7 @@ def parse_args():
     p.add_argument("--ozaki-stack", type=int, default=200000, help="triples per stack of the ozaki workload")
     p.add_argument("--gemm-sizes", default="2048,4096,8192,16384", help="square sizes of the gemm workload")
     p.add_argument("--gemm-slices", default="5,6,7,8", help="slice counts of the gemm workload")
+    p.add_argument("--gemm-moduli", default="0", help="modulus counts of the scheme-2 (CRT) GEMM (0: full precision)")
     return p.parse_args()
 
 
@@ -333,6 +334,17 @@ def run_b200(args, d: Dist):
             traffic = json.loads(tfile.read_text()).get("smm_23x23x23_s30000")
         except (OSError, ValueError):
             traffic = None
+    # the stated contract's roofline for this workload: min(FP64 peak, HBM bandwidth x arithmetic
+    # intensity of the reference's byte formula), HBM from MEASURED_PEAKS.json
+    hbm_gbs, hbm_src = 6650.0, "fallback 6.65 TB/s"
+    pfile = ROOT / "MEASURED_PEAKS.json"
+    if pfile.exists():
+        try:
+            hbm_gbs, hbm_src = float(json.loads(pfile.read_text())["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+        except (OSError, ValueError, KeyError):
+            pass
+    ai = case.flops / (8.0 * S * (m * k + k * n + 2.0 * m * n))
+    contract_tf = min(peak or float("inf"), hbm_gbs * ai * 1e-3)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved and peak and peak > 0 else None, "traffic": traffic,
                 "kernel": "xs_smm_staged_kernel<23,23,23,2> (stack kernel of this shape)",
@@ -340,7 +352,13 @@ def run_b200(args, d: Dist):
                 "(libxstream_b200_fp64_peak: mma.sync m8n8k4 f64 loop)",
                 "reference_bytes_rate_gbs": (smm["gbyte"] / smm["ms"] * 1e3) if smm else None,
                 "note": "A/B/C pools (39 MB) fit in L2; the reference's byte statement S*8*(mk+kn+2mn) "
-                        "counts every operand from DRAM, so the FP64 pipe, not HBM, bounds this kernel"}
+                        "counts every operand from DRAM, so the FP64 pipe, not HBM, bounds this kernel",
+                "hbm_ai_roofline": {"tflops": contract_tf, "hbm_gbs": hbm_gbs, "hbm_source": hbm_src,
+                                    "flop_per_byte": ai, "frac_step": (value * 1e-3) / contract_tf,
+                                    "frac_kernel": (achieved / contract_tf) if achieved else None,
+                                    "note": "min(FP64 peak, HBM GB/s x flops per reference-formula byte): the "
+                                            "roofline the workload's statement uses; above 1 because the pools "
+                                            "stay in L2"}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": value / V100_PUBLISHED,
@@ -578,16 +596,31 @@ def run_gemm(args, d: Dist):
                                 "int8_tops": npairs * flops / ms * 1e-9, "relerr": err,
                                 "speedup_vs_plain": ms_plain / ms})
             entry["ozaki"] = ozk
+            crt = []
+            for nm in [int(x) for x in args.gemm_moduli.split(",") if x]:
+                def oz2():
+                    xs.check(L.libxstream_b200_ozaki2_gemm(b"N", b"N", N, N, N, 1.0, av.data_ptr(), N, b.data_ptr(), N,
+                                                           0.0, c.data_ptr(), N, nm, sh), "ozaki2_gemm")
+                ms = timed(oz2)
+                diff = (c - c_ref).view(N, N).abs()
+                if variant == "uniform":
+                    err = float(diff.max() / c_ref.abs().max())
+                else:
+                    err = float((diff.amax(dim=0) / ref_rows.clamp_min(1e-300)).max())
+                nmod = nm if nm else int(L.xs_ozaki2_default_moduli(N)) if hasattr(L, "xs_ozaki2_default_moduli") else nm
+                crt.append({"moduli": nmod, "ms": ms, "tflops_fp64_equiv": flops / ms * 1e-9,
+                            "int8_tops": nmod * flops / ms * 1e-9, "relerr": err, "speedup_vs_plain": ms_plain / ms})
+            entry["ozaki2_crt"] = crt
             results.append(entry)
         del a, b, a_rs, c, c_ref
         torch.cuda.empty_cache()
     clocks = sampler.stop()
     best = None
     for e in results:
-        for o in e["ozaki"]:
+        for o in e["ozaki"] + e.get("ozaki2_crt", []):
             if o["relerr"] <= 1e-13 and (best is None or (e["N"], o["tflops_fp64_equiv"]) > (best[0], best[1]["tflops_fp64_equiv"])):
                 best = (e["N"], o, e["plain_dmma"]["tflops"])
-    line = {"metric": "dense FP64 GEMM TFLOP/s (FP64-equivalent), Ozaki int8 tensor-core form vs plain DMMA",
+    line = {"metric": "dense FP64 GEMM TFLOP/s (FP64-equivalent), Ozaki int8 tensor-core forms (slices, CRT) vs plain DMMA",
             "value": best[1]["tflops_fp64_equiv"] if best else None, "unit": "TFLOP/s", "n_gpus": 1,
             "steps": steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64 (int8 slices)",
             "data": "synthetic", "config": {"workload": "square dense GEMM, N in " + args.gemm_sizes,

@@ -130,6 +130,20 @@ int libxstream_b200_ozaki_gemm(char transa, char transb, int M, int N, int K, do
   const double* b, int ldb, double beta, double* c, int ldc, int nslices, int trim, void* stream);
 
 /**
+ * Ozaki scheme-2 (Chinese remainder) FP64 GEMM on the int8 tensor cores: C = alpha*op(A)*op(B) +
+ * beta*C with column-major device operands (op = 'N' or 'T'). Rows of op(A) / columns of op(B) are
+ * scaled by their largest power of two and truncated to integers, whose product is computed modulo
+ * nmoduli pairwise coprime moduli <= 256 (one unsigned 8-bit tensor-core GEMM each, exact int32 sums)
+ * and reconstructed by the CRT in double-double arithmetic. nmoduli 1..20 sets the precision (inputs
+ * keep floor((log2 P - log2 K - 2) / 2) bits, at most 53); 0 takes the fewest moduli that keep all 53
+ * (16 for K <= 4096). Replaces ozaki_gemm for Scheme 2 (samples/ozaki/ozaki_opencl.h:420-421 with
+ * ozaki_init kind 2, ozaki_opencl.h:321-329; nmoduli plays the role of ndecomp). Enqueued on stream
+ * (NULL: the per-thread default stream); returns 0 on success.
+ */
+int libxstream_b200_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
+  const double* b, int ldb, double beta, double* c, int ldc, int nmoduli, void* stream);
+
+/**
  * Plain FP64 GEMM on the FP64 tensor cores (DMMA): C = alpha*A*B + beta*C, column-major device
  * operands, transa = transb = 'N' only (other values return nonzero). The baseline for
  * libxstream_b200_ozaki_gemm; no counterpart in the reference (which compares with host DGEMM).

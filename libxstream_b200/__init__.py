@@ -87,6 +87,10 @@ SIGNATURES = {
                                                   ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                   ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
                                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "libxstream_b200_ozaki2_gemm": (ctypes.c_int, [ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                   ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_void_p]),
     "libxstream_b200_dgemm": (ctypes.c_int, [ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),

@@ -166,6 +166,13 @@ def ozaki_gemm(transa: str, transb: str, M: int, N: int, K: int, alpha: float, a
                                             beta, c.ptr, ldc, nslices, trim, stream.handle if stream else None)
 
 
+def ozaki2_gemm(transa: str, transb: str, M: int, N: int, K: int, alpha: float, a: DevBuf, lda: int, b: DevBuf,
+                ldb: int, beta: float, c: DevBuf, ldc: int, nmoduli: int = 0, stream: Stream | None = None) -> int:
+    """libxstream_b200_ozaki2_gemm: C = alpha*op(A)*op(B) + beta*C by the CRT scheme (column-major, device buffers)."""
+    return lib().libxstream_b200_ozaki2_gemm(transa.encode(), transb.encode(), M, N, K, alpha, a.ptr, lda, b.ptr, ldb,
+                                             beta, c.ptr, ldc, nmoduli, stream.handle if stream else None)
+
+
 def dgemm(M: int, N: int, K: int, alpha: float, a: DevBuf, lda: int, b: DevBuf, ldb: int, beta: float, c: DevBuf,
           ldc: int, stream: Stream | None = None) -> int:
     """libxstream_b200_dgemm (plain FP64 DMMA GEMM, 'N', 'N')."""

@@ -23,7 +23,7 @@ LIB = OUT_DIR / "libxstream_b200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 C_SOURCES = ["acc_runtime.c", "smm_params.c", "smm_acc.c", "profile.c", "gemm_api.c", "predictor.c", "offload_cp2k.c"]
-CU_SOURCES = ["smm_kernels.cu", "stack_sort.cu", "smm_noalloc.cu", "ozaki_gemm.cu", "dgemm.cu", "ozaki_smm.cu", "tune.cu", "mlp.cu"]
+CU_SOURCES = ["smm_kernels.cu", "stack_sort.cu", "smm_noalloc.cu", "ozaki_gemm.cu", "ozaki2_gemm.cu", "dgemm.cu", "ozaki_smm.cu", "tune.cu", "mlp.cu"]
 
 
 def _nvcc() -> str:

@@ -27,6 +27,22 @@ int libxstream_b200_ozaki_gemm(char transa, char transb, int M, int N, int K, do
   return xs_record_error(r, "ozaki_gemm");
 }
 
+int libxstream_b200_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
+  const double* b, int ldb, double beta, double* c, int ldc, int nmoduli, void* stream) {
+  void* scratch = NULL;
+  size_t nbytes;
+  int r;
+  if (EXIT_SUCCESS != xs_smm_ensure_init()) return EXIT_FAILURE;
+  if (NULL == stream) stream = xs_default_stream();
+  if (0 > nmoduli || 20 < nmoduli) return xs_record_error(1, "ozaki2_gemm: nmoduli outside 0..20");
+  if (0 == nmoduli) nmoduli = xs_ozaki2_default_moduli(K); /* full FP64 input precision for this K */
+  nbytes = (0 < M && 0 < N && 0 < K && 0.0 != alpha) ? xs_ozaki2_gemm_scratch_bytes(M, N, K, nmoduli) : 0;
+  if (0 < nbytes && EXIT_SUCCESS != xs_scratch_alloc(&scratch, nbytes, stream)) return EXIT_FAILURE;
+  r = xs_ozaki2_gemm(transa, transb, M, N, K, alpha, a, lda, b, ldb, beta, c, ldc, nmoduli, scratch, nbytes, stream);
+  if (NULL != scratch) xs_scratch_free(scratch, stream);
+  return xs_record_error(r, "ozaki2_gemm");
+}
+
 int libxstream_b200_dgemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda,
   const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
   if (EXIT_SUCCESS != xs_smm_ensure_init()) return EXIT_FAILURE;

@@ -100,6 +100,14 @@ size_t xs_ozaki_gemm_scratch_bytes(int M, int N, int K, int nslices);
 int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda, const double* b,
   int ldb, double beta, double* c, int ldc, int nslices, int cutoff, void* scratch, size_t scratch_bytes, void* stream);
 
+/** Ozaki scheme-2 (CRT) FP64 GEMM on the int8 tensor cores (ozaki2_gemm.cu): C = alpha*op(A)*op(B) +
+    beta*C, column-major, nmod moduli (1..20; 0: the fewest that keep all 53 bits for this K).
+    scratch must hold xs_ozaki2_gemm_scratch_bytes(). Returns a cudaError_t value. */
+int xs_ozaki2_default_moduli(int K);
+size_t xs_ozaki2_gemm_scratch_bytes(int M, int N, int K, int nmod);
+int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda, const double* b,
+  int ldb, double beta, double* c, int ldc, int nmod, void* scratch, size_t scratch_bytes, void* stream);
+
 /** Ozaki scheme-1 stack multiply (ozaki_smm.cu): C[c] += A[a]*B[b] for one shape m, n, k <= 64 with
     int8 tensor-core slice products; A pool of na m x k column-major blocks, B pool of nb k x n
     row-major blocks, 1-based block-aligned offsets. Returns a cudaError_t value. */

@@ -1,0 +1,592 @@
+/*
+ * Ozaki scheme-2 FP64 GEMM on the int8 tensor cores: Chinese-remainder (CRT) form.
+ *
+ * C = alpha * op(A) * op(B) + beta * C, FP64, column-major (BLAS conventions), the second scheme of
+ * the reference's Ozaki sample (samples/ozaki/kernels/ozaki2_int8.cl:13-45, host set-up
+ * samples/ozaki/ozaki_opencl.c:415-460). Each row of op(A) and each column of op(B) is scaled by its
+ * largest power of two and turned into integers of MB bits (the aligned significands of
+ * xs_oz::ieee_split, truncated to MB bits; MB = 53 keeps every bit of the largest entry). The exact
+ * integer product A_int * B_int is then computed modulo q moduli m_1..m_q (pairwise coprime, at most
+ * 256, so residues are unsigned bytes): one unsigned 8-bit GEMM per modulus on the tensor cores
+ * (tcgen05.mma kind::i8, u8 x u8 -> exact int32 sums over up to 32768 k, reduced modulo m_i in the
+ * epilogue and kept as one byte per modulus and output), and the integer is reconstructed from its
+ * residues by the CRT with the "fractional" formula
+ *     x / P = frac( sum_i r_i * y_i / m_i ),   P = prod m_i,  y_i = (P / m_i)^-1 mod m_i,
+ * evaluated in double-double arithmetic (Dekker's two-product with an FMA and Knuth's two-sum),
+ * centred to [-P/2, P/2) and scaled back: C(i,j) = x * 2^(ea_i + eb_j - 2150 + 2 (53 - MB)).
+ * The modulus count decides the precision: P must exceed 2 K 2^(2 MB), so q moduli carry
+ * MB = floor((log2 P - ceil(log2 K) - 2) / 2) bits per input (capped at 53); the default takes the fewest
+ * moduli that give MB = 53 for this K (16 up to K = 2^17).
+ *
+ * Device layout: residue planes rA[q][M][Kp] and rB[q][N][Kp] (u8, K contiguous, zero padded),
+ * exponents ea[M], eb[N], residues of C R[q][N][M] (u8, column-major per modulus).
+ *
+ * GEMM kernel: one CTA per 128 x 256 tile of C, 6 warps, the pipeline of the scheme-1 kernel with
+ * one accumulation group per modulus: warp 0 streams (modulus, k-block) tiles of both operands into
+ * a 4-stage shared-memory ring with TMA (128-byte swizzle); warp 1 owns two 128 x 256 int32
+ * accumulators in tensor memory and one lane issues the MMAs; warps 2-5 reduce a finished
+ * accumulator modulo m_i and store the bytes while the tensor cores work on the next modulus. Every
+ * mbarrier wait is bounded (per-call abort word, library device error word).
+ */
+#include "internal.h"
+#include "tc_ptx.cuh"
+#include "ozaki_digits.cuh"
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+extern "C" unsigned* xs_device_error_ptr(void);
+
+namespace {
+using namespace xs_tc;
+using namespace xs_oz;
+
+constexpr int kMaxMod = 20;
+constexpr int kBM = 128, kBN = 256, kBK = 128, kStages = 4;
+constexpr int kThreads = 192;
+constexpr int kGroupM = 8;
+/* k-blocks per launch: 32768 * 255^2 < 2^31 keeps every int32 sum exact */
+constexpr int kKChunkBlocks = 32768 / kBK;
+constexpr int kATileBytes = kBM * kBK, kBTileBytes = kBN * kBK;
+constexpr unsigned kErrOzakiTimeout = 4u;
+
+/* Pairwise coprime moduli <= 256, largest first (products of primes where composite). */
+constexpr unsigned kModuli[kMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                       223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+
+struct Oz2Consts {
+  unsigned mod[kMaxMod];
+  unsigned long long inv64[kMaxMod]; /* floor(2^64 / m_i) + 1: floor(u / m_i) = umulhi64(u, inv64) for u < 2^53 */
+  double whi[kMaxMod], wlo[kMaxMod]; /* y_i / m_i as a double-double */
+  double phi, plo; /* P as a double-double */
+  int nmod, mb;
+};
+
+/* --------------------------------------------------------------------------- preprocessing */
+
+/* Row maxima of the biased exponent, rows contiguous (element (r, k) at x[r + k*ld]); partial
+   maxima meet in emax[] (zeroed by the caller) by atomicMax. */
+__global__ void xs_oz2_rowexp_rc(const double* __restrict__ x, long long ld, int R, int K, int kchunk, int* __restrict__ emax) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const int k0 = blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
+  int e = 0;
+  for (int k = k0; k < k1; ++k) e = max(e, biased_exp(x[r + (long long)k * ld]));
+  if (0 != e) atomicMax(emax + r, e);
+}
+
+/* Row maxima with k contiguous (element (r, k) at x[k + r*ld]); one warp per row. */
+__global__ void xs_oz2_rowexp_kc(const double* __restrict__ x, long long ld, int R, int K, int* __restrict__ emax) {
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (r >= R) return;
+  const double* const row = x + (long long)r * ld;
+  int e = 0;
+  for (int k = lane; k < K; k += 32) e = max(e, biased_exp(row[k]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if (0 == lane) emax[r] = e;
+}
+
+/* |v| scaled to the row's largest exponent and truncated to mb bits, and its sign. */
+__device__ __forceinline__ unsigned long long aligned_int(double v, int erow, int mb, unsigned& sign) {
+  int be;
+  unsigned long long mt;
+  ieee_split(v, sign, be, mt);
+  const int sh = erow - be + 53 - mb;
+  return (0 != mt && sh < 64) ? (mt >> sh) : 0ull;
+}
+
+/* u mod m for u < 2^53 and m <= 256 from inv = floor(2^64 / m) + 1: the high product is
+   u/m + u*e/2^64 with 0 < e < 1, and since u/m is at most (m-1)/m <= 1 - 2^-8 above an integer
+   and u*e/2^64 < 2^-11, its integer part is floor(u / m) exactly. */
+__device__ __forceinline__ unsigned mod_small(unsigned long long u, unsigned m, unsigned long long inv) {
+  return (unsigned)(u - __umul64hi(u, inv) * m);
+}
+
+/* Residue of the signed integer (-1)^sign * u (u < 2^53) modulo m, in [0, m). */
+__device__ __forceinline__ unsigned residue(unsigned long long u, unsigned sign, unsigned m, unsigned long long inv) {
+  const unsigned x = (256u == m) ? ((unsigned)u & 255u) : mod_small(u, m, inv);
+  return (sign && 0u != x) ? m - x : x;
+}
+
+/* Residues of 16 consecutive k of one row into the planes d[i][r][k0 .. k0+15]. */
+__device__ __forceinline__ void residues16(const double (&v)[16], int erow, const Oz2Consts& cs, unsigned char* __restrict__ d,
+  long long plane, long long off) {
+  unsigned long long u[16];
+  unsigned sg[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) u[j] = aligned_int(v[j], erow, cs.mb, sg[j]);
+  for (int i = 0; i < cs.nmod; ++i) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t x = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) x |= residue(u[q * 4 + b], sg[q * 4 + b], cs.mod[i], cs.inv64[i]) << (8 * b);
+      w[q] = x;
+    }
+    *reinterpret_cast<uint4*>(d + i * plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+/* k contiguous (element (r, k) at x[k + r*ld]): one thread per (row, 16 k). */
+__global__ void xs_oz2_res_kc(const double* __restrict__ x, long long ld, int R, int K, int Kp, const int* __restrict__ emax,
+  const __grid_constant__ Oz2Consts cs, unsigned char* __restrict__ d) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int kg = Kp / 16;
+  if (t >= (long long)R * kg) return;
+  const int r = (int)(t / kg), k0 = (int)(t - (long long)r * kg) * 16;
+  const double* const row = x + (long long)r * ld;
+  double v[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? row[k0 + j] : 0.0;
+  residues16(v, emax[r], cs, d, (long long)R * Kp, (long long)r * Kp + k0);
+}
+
+/* rows contiguous (element (r, k) at x[r + k*ld]): threads over rows, blockIdx.y over 16 k. */
+__global__ void xs_oz2_res_rc(const double* __restrict__ x, long long ld, int R, int K, int Kp, const int* __restrict__ emax,
+  const __grid_constant__ Oz2Consts cs, unsigned char* __restrict__ d) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const int k0 = blockIdx.y * 16;
+  double v[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? x[r + (long long)(k0 + j) * ld] : 0.0;
+  residues16(v, emax[r], cs, d, (long long)R * Kp, (long long)r * Kp + k0);
+}
+
+/* C = beta * C (K == 0 or alpha == 0). */
+__global__ void xs_oz2_scale_c(double* __restrict__ c, long long ldc, int M, int N, double beta) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)M * N) return;
+  const long long j = t / M, i = t - j * M;
+  double* const p = c + i + j * ldc;
+  *p = (0.0 == beta) ? 0.0 : beta * *p;
+}
+
+/* ------------------------------------------------------------------------------------ GEMM */
+
+struct Oz2GemmArgs {
+  int M, N, kb0, kb1; /* k-blocks [kb0, kb1) of 128 */
+  int nmod;
+  int first; /* 1: the first k-chunk (residues are written, not accumulated) */
+  unsigned mod[kMaxMod];
+  unsigned long long inv64[kMaxMod];
+  unsigned char* R; /* [nmod][N][M] */
+  unsigned* abort;
+  unsigned* dev_err;
+};
+
+constexpr size_t gemm_smem_bytes() {
+  return 1024 /* alignment slack */ + (size_t)kStages * (kATileBytes + kBTileBytes) + 16 * sizeof(uint64_t) + 16;
+}
+
+/* instruction descriptor of tcgen05.mma kind::i8 with unsigned 8-bit A and B, s32 accumulator */
+__host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {
+  return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+  xs_ozaki2_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+    const __grid_constant__ Oz2GemmArgs args) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* const smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* const sA = smem;
+  unsigned char* const sB = smem + kStages * kATileBytes;
+  uint64_t* const bars = (uint64_t*)(sB + kStages * kBTileBytes);
+  uint64_t* const full = bars;
+  uint64_t* const empty = bars + kStages;
+  uint64_t* const accf = bars + 2 * kStages;
+  uint64_t* const acce = accf + 2;
+  uint32_t* const tmem_slot = (uint32_t*)(bars + 16);
+  unsigned* const abort = args.abort;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int n0, m0; /* grouped rasterization: kGroupM row panels sweep the column panels together */
+  {
+    const int ntm = (args.M + kBM - 1) / kBM, ntn = (args.N + kBN - 1) / kBN;
+    const int id = blockIdx.x, per_group = kGroupM * ntn, g = id / per_group, first = g * kGroupM;
+    const int gsize = min(kGroupM, ntm - first), r = id - g * per_group;
+    m0 = (first + r % gsize) * kBM;
+    n0 = (r / gsize) * kBN;
+  }
+  if (0 == threadIdx.x) {
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&accf[i], 1);
+      mbar_init(&acce[i], 128);
+    }
+    fence_barrier_init();
+    prefetch_tensormap(&mapA);
+    prefetch_tensormap(&mapB);
+  }
+  if (1 == warp) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (0 == warp) { /* TMA producer */
+    if (0 == lane) {
+      int it = 0;
+      bool ok = true;
+      for (int q = 0; q < args.nmod && ok; ++q) {
+        for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+          if (!(ok = mbar_wait(&empty[stage], ph ^ 1u, abort, 1u))) break;
+          mbar_arrive_expect_tx(&full[stage], kATileBytes + kBTileBytes);
+          tma_load_3d(sA + stage * kATileBytes, &mapA, kb * kBK, m0, q, &full[stage]);
+          tma_load_3d(sB + stage * kBTileBytes, &mapB, kb * kBK, n0, q, &full[stage]);
+        }
+      }
+    }
+  }
+  else if (1 == warp) { /* MMA issuer */
+    if (0 == lane) {
+      const uint32_t idesc = idesc_u8(kBM, kBN);
+      int it = 0;
+      bool ok = true;
+      for (int q = 0; q < args.nmod && ok; ++q) {
+        const int buf = q & 1, use = q >> 1;
+        if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u))) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(buf * kBN);
+        uint32_t acc = 0;
+        for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+          if (!(ok = mbar_wait(&full[stage], ph, abort, 2u))) break;
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + stage * kATileBytes), b0 = smem_u32(sB + stage * kBTileBytes);
+#pragma unroll
+          for (int kk = 0; kk < kBK / 32; ++kk) {
+            mma_i8(d, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), idesc, acc);
+            acc = 1;
+          }
+          mma_commit(&empty[stage]);
+        }
+        if (ok) mma_commit(&accf[buf]);
+      }
+    }
+  }
+  else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; thread = one row of the tile */
+    const int qd = warp & 3;
+    const int row = m0 + qd * 32 + lane;
+    const bool rok = row < args.M;
+    for (int q = 0; q < args.nmod; ++q) {
+      const int buf = q & 1, use = q >> 1;
+      if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u)) break;
+      tc_fence_after();
+      const unsigned m = args.mod[q];
+      const unsigned long long inv = args.inv64[q];
+      unsigned char* const plane = args.R + (size_t)q * args.M * args.N;
+      for (int c0 = 0; c0 < kBN; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(buf * kBN + c0), v);
+        tmem_ld_wait();
+        if (rok) {
+          const int ncol = min(32, args.N - (n0 + c0));
+          unsigned char* const dst = plane + row + (size_t)(n0 + c0) * args.M;
+          unsigned prev[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) prev[j] = (j < ncol && !args.first) ? dst[(size_t)j * args.M] : 0u;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            if (j < ncol) dst[(size_t)j * args.M] = (unsigned char)mod_small((unsigned long long)v[j] + prev[j], m, inv);
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+    }
+  }
+  if (0 != *(volatile unsigned*)abort) { /* let copies and MMAs still in flight land before TMEM goes */
+    for (int i = 0; i < 200; ++i) __nanosleep(1000);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (1 == warp) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+  if (0 == threadIdx.x && 0 != *(volatile unsigned*)abort) atomicOr(args.dev_err, kErrOzakiTimeout);
+}
+
+/* ---------------------------------------------------------------------------- reconstruction */
+
+/* Knuth's two-sum and Dekker's two-product (with an FMA): s + e == a + b, p + e == a * b exactly. */
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+/* C(i,j) = alpha * x * 2^E + beta * C(i,j), x the centred integer with residues R[.][j][i]. One
+   thread per element, consecutive threads on consecutive rows. */
+__global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* __restrict__ R, int M, int N,
+  const int* __restrict__ ea, const int* __restrict__ eb, const __grid_constant__ Oz2Consts cs, double alpha, double beta,
+  double* __restrict__ C, long long ldc) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)M * N) return;
+  const int j = (int)(t / M), i = (int)(t - (long long)j * M);
+  const size_t plane = (size_t)M * N, off = (size_t)j * M + i;
+  /* s = frac(sum_q r_q * w_q), kept in [0, 1) as a double-double */
+  double sh = 0.0, sl = 0.0;
+  for (int q = 0; q < cs.nmod; ++q) {
+    const double r = (double)R[(size_t)q * plane + off];
+    const double p = r * cs.whi[q];
+    const double pe = fma(r, cs.whi[q], -p) + r * cs.wlo[q];
+    double s, e;
+    two_sum(sh, p, s, e);
+    e += sl + pe;
+    sh = s + e;
+    sl = e - (sh - s);
+    const double f = floor(sh);
+    sh -= f; /* exact: sh < 2^10 */
+    two_sum(sh, sl, s, e);
+    sh = s;
+    sl = e;
+  }
+  if (sh + sl < 0.0) sh += 1.0;
+  if (sh + sl >= 0.5) sh -= 1.0; /* centre: x in [-P/2, P/2) */
+  const double x = fma(sh, cs.phi, fma(sh, cs.plo, sl * cs.phi));
+  const int ia = ea[i], ib = eb[j];
+  double v = 0.0;
+  if (0 != ia && 0 != ib) v = ldexp(x, ia + ib - 2150 + 2 * (53 - cs.mb));
+  double* const cp = C + i + (long long)j * ldc;
+  *cp = (0.0 == beta) ? alpha * v : fma(alpha, v, beta * *cp);
+}
+
+/* ------------------------------------------------------------------------------------ host */
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn(void) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (nullptr == fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaSuccess == cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) &&
+        cudaDriverEntryPointSuccess == q) {
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+  }
+  return fn;
+}
+
+/* 3-D map over residue planes d[q][R][Kp] (u8), box 128 (k) x rows x 1, 128-byte swizzle. */
+int make_plane_map(CUtensorMap* map, const void* base, int Kp, int R, int nq, int box_rows) {
+  const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+  if (nullptr == fn) return (int)cudaErrorNotSupported;
+  const cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)R, (cuuint64_t)nq};
+  const cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * (cuuint64_t)R};
+  const cuuint32_t box[3] = {(cuuint32_t)kBK, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
+    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (CUDA_SUCCESS == r) ? 0 : (int)cudaErrorInvalidValue;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+unsigned gcd_host(unsigned a, unsigned b) {
+  while (0 != b) {
+    const unsigned t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+/* inverse of a modulo m (gcd(a, m) == 1), extended Euclid */
+unsigned inv_mod(unsigned a, unsigned m) {
+  long long t = 0, nt = 1, r = m, nr = a % m;
+  while (0 != nr) {
+    const long long q = r / nr, tt = t - q * nt, rr = r - q * nr;
+    t = nt;
+    nt = tt;
+    r = nr;
+    nr = rr;
+  }
+  return (unsigned)((t % (long long)m + (long long)m) % (long long)m);
+}
+
+/* log2 of the product of the first n moduli */
+double log2_product(int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += log2((double)kModuli[i]);
+  return s;
+}
+
+/* Constants of the CRT with the first nmod moduli for inner dimension K. Returns the mantissa bits
+   the inputs keep (0 if nmod cannot hold even one bit). */
+int make_consts(int nmod, int K, Oz2Consts* cs) {
+  memset(cs, 0, sizeof(*cs));
+  cs->nmod = nmod;
+  for (int i = 0; i < nmod; ++i) {
+    for (int j = 0; j < i; ++j) {
+      if (1u != gcd_host(kModuli[i], kModuli[j])) return 0;
+    }
+  }
+  /* P as a 128-bit integer (product of at most 20 factors <= 2^8 fits up to 16 factors exactly;
+     beyond that only the double-double value of P matters, computed by scaling) */
+  unsigned __int128 P = 1;
+  long double Pld = 1.0L;
+  for (int i = 0; i < nmod; ++i) {
+    Pld *= (long double)kModuli[i];
+    if (i < 16) P *= kModuli[i];
+  }
+  if (nmod <= 16) {
+    cs->phi = (double)P;
+    const unsigned __int128 hi = (unsigned __int128)cs->phi;
+    cs->plo = (P >= hi) ? (double)(P - hi) : -(double)(hi - P);
+  }
+  else {
+    cs->phi = (double)Pld;
+    cs->plo = (double)(Pld - (long double)cs->phi);
+  }
+  for (int i = 0; i < nmod; ++i) {
+    const unsigned m = kModuli[i];
+    unsigned pm = 1; /* (P / m) mod m */
+    for (int j = 0; j < nmod; ++j) {
+      if (j != i) pm = (unsigned)(((unsigned long long)pm * (kModuli[j] % m)) % m);
+    }
+    const unsigned y = inv_mod(pm, m);
+    cs->mod[i] = m;
+    cs->inv64[i] = (256u == m) ? 0ull : (unsigned long long)(((unsigned __int128)1 << 64) / m) + 1ull;
+    cs->whi[i] = (double)y / (double)m;
+    cs->wlo[i] = fma(-cs->whi[i], (double)m, (double)y) / (double)m; /* the remainder y - whi*m is exact */
+  }
+  int lgk = 0;
+  while ((1ll << lgk) < (long long)K) ++lgk;
+  const int mb = (int)floor((log2_product(nmod) - 1.0 - lgk - 1.0) / 2.0);
+  cs->mb = (mb > 53) ? 53 : mb;
+  return (cs->mb > 0) ? cs->mb : 0;
+}
+
+/* Fewest moduli that keep all 53 bits for inner dimension K. */
+int default_nmod(int K) {
+  int lgk = 0;
+  while ((1ll << lgk) < (long long)K) ++lgk;
+  for (int n = 1; n <= kMaxMod; ++n) {
+    if (log2_product(n) - 1.0 >= 2.0 * 53 + lgk + 1.0) return n;
+  }
+  return kMaxMod;
+}
+
+int residue_operand(const double* x, long long ld, bool rows_contiguous, int R, int K, int Kp, const Oz2Consts& cs, int* emax,
+  unsigned char* planes, cudaStream_t s) {
+  if (rows_contiguous) {
+    const int kchunk = 256;
+    xs_oz2_rowexp_rc<<<dim3((R + 255) / 256, (K + kchunk - 1) / kchunk), 256, 0, s>>>(x, ld, R, K, kchunk, emax);
+    xs_oz2_res_rc<<<dim3((R + 127) / 128, Kp / 16), 128, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
+  }
+  else {
+    xs_oz2_rowexp_kc<<<(R + 7) / 8, 256, 0, s>>>(x, ld, R, K, emax);
+    const long long n = (long long)R * (Kp / 16);
+    xs_oz2_res_kc<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
+  }
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+int xs_ozaki2_default_moduli(int K) { return default_nmod(K > 0 ? K : 1); }
+
+size_t xs_ozaki2_gemm_scratch_bytes(int M, int N, int K, int nmod) {
+  if (nmod <= 0) nmod = default_nmod(K > 0 ? K : 1);
+  const size_t Kp = align_up((size_t)(K > 0 ? K : 1), 16);
+  return align_up((size_t)nmod * M * Kp, 1024) + align_up((size_t)nmod * N * Kp, 1024) + align_up((size_t)nmod * M * N, 1024) +
+         align_up(sizeof(int) * M, 256) + align_up(sizeof(int) * N, 256) + 256;
+}
+
+int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, const double* a, int lda, const double* b,
+  int ldb, double beta, double* c, int ldc, int nmod, void* scratch, size_t scratch_bytes, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool ta = ('T' == transa || 't' == transa || 'C' == transa || 'c' == transa);
+  const bool tb = ('T' == transb || 't' == transb || 'C' == transb || 'c' == transb);
+  if (M < 0 || N < 0 || K < 0 || nmod < 0 || nmod > kMaxMod || ldc < (M > 1 ? M : 1)) return (int)cudaErrorInvalidValue;
+  if (0 == M || 0 == N) return 0;
+  if (0 == K || 0.0 == alpha) {
+    if (1.0 == beta) return 0;
+    const long long n = (long long)M * N;
+    xs_oz2_scale_c<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(c, ldc, M, N, beta);
+    return (int)cudaGetLastError();
+  }
+  if (lda < (ta ? K : M) || ldb < (tb ? N : K)) return (int)cudaErrorInvalidValue;
+  if (0 == nmod) nmod = default_nmod(K);
+  Oz2Consts cs;
+  if (0 == make_consts(nmod, K, &cs)) return (int)cudaErrorInvalidValue; /* too few moduli for this K */
+  if (nullptr == scratch || scratch_bytes < xs_ozaki2_gemm_scratch_bytes(M, N, K, nmod)) return (int)cudaErrorInvalidValue;
+  const int Kp = (int)align_up((size_t)K, 16);
+  char* p = (char*)scratch;
+  unsigned char* const rA = (unsigned char*)p;
+  p += align_up((size_t)nmod * M * Kp, 1024);
+  unsigned char* const rB = (unsigned char*)p;
+  p += align_up((size_t)nmod * N * Kp, 1024);
+  unsigned char* const rC = (unsigned char*)p;
+  p += align_up((size_t)nmod * M * N, 1024);
+  int* const ea = (int*)p;
+  p += align_up(sizeof(int) * M, 256);
+  int* const eb = (int*)p;
+  p += align_up(sizeof(int) * N, 256);
+  unsigned* const abort = (unsigned*)p;
+  int r = (int)cudaMemsetAsync(ea, 0, (size_t)(p - (char*)ea) + 256, s);
+  if (0 != r) return r;
+  void* prof = xs_profile_begin(stream);
+  if (0 != (r = residue_operand(a, lda, !ta, M, K, Kp, cs, ea, rA, s))) return r;
+  if (0 != (r = residue_operand(b, ldb, tb, N, K, Kp, cs, eb, rB, s))) return r;
+  xs_profile_end(prof, "ozaki2_residues", 0.0, 8.0 * ((double)M * K + (double)K * N), stream);
+  CUtensorMap mapA, mapB;
+  if (0 != (r = make_plane_map(&mapA, rA, Kp, M, nmod, kBM))) return r;
+  if (0 != (r = make_plane_map(&mapB, rB, Kp, N, nmod, kBN))) return r;
+  Oz2GemmArgs args;
+  memset(&args, 0, sizeof(args));
+  args.M = M;
+  args.N = N;
+  args.nmod = nmod;
+  for (int i = 0; i < nmod; ++i) {
+    args.mod[i] = cs.mod[i];
+    args.inv64[i] = cs.inv64[i];
+  }
+  args.R = rC;
+  args.abort = abort;
+  args.dev_err = xs_device_error_ptr();
+  if (nullptr == args.dev_err) return (int)cudaErrorInvalidValue;
+  const size_t smem = gemm_smem_bytes();
+  static int smem_set = 0;
+  if (!smem_set) {
+    if (0 != (r = (int)cudaFuncSetAttribute(xs_ozaki2_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return r;
+    smem_set = 1;
+  }
+  const int nkb = (K + kBK - 1) / kBK;
+  const dim3 grid(((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM));
+  for (int kb0 = 0; kb0 < nkb; kb0 += kKChunkBlocks) {
+    args.kb0 = kb0;
+    args.kb1 = (kb0 + kKChunkBlocks < nkb) ? kb0 + kKChunkBlocks : nkb;
+    args.first = (0 == kb0) ? 1 : 0;
+    prof = xs_profile_begin(stream);
+    xs_ozaki2_gemm_kernel<<<grid, kThreads, smem, s>>>(mapA, mapB, args);
+    if (0 != (r = (int)cudaGetLastError())) return r;
+    const double kc = (double)(args.kb1 - args.kb0) * kBK;
+    xs_profile_end(prof, "ozaki2_gemm", 2.0 * M * N * (kc < K ? kc : K), 0.0, stream);
+  }
+  prof = xs_profile_begin(stream);
+  const long long n = (long long)M * N;
+  xs_oz2_reconstruct<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rC, M, N, ea, eb, cs, alpha, beta, c, ldc);
+  r = (int)cudaGetLastError();
+  xs_profile_end(prof, "ozaki2_reconstruct", 0.0, (double)nmod * n + 16.0 * n, stream);
+  return r;
+}
+
+}  // extern "C"
