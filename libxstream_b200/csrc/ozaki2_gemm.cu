@@ -59,9 +59,14 @@ constexpr unsigned kModuli[kMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 2
 struct Oz2Consts {
   unsigned mod[kMaxMod];
   unsigned long long inv64[kMaxMod]; /* floor(2^64 / m_i) + 1: floor(u / m_i) = umulhi64(u, inv64) for u < 2^53 */
-  double whi[kMaxMod], wlo[kMaxMod]; /* y_i / m_i as a double-double */
   double phi, plo; /* P as a double-double */
   int nmod, mb;
+  /* reconstruction over moduli pairs (m_2p, m_2p+1), combined first into one residue modulo their
+     product (a last unpaired modulus has pb = 1): pinv = m_2p^-1 mod m_2p+1, w = y / (m_2p m_2p+1) */
+  int npair;
+  unsigned pa[kMaxMod / 2], pb[kMaxMod / 2], pinv[kMaxMod / 2];
+  unsigned long long pbinv64[kMaxMod / 2];
+  double whi[kMaxMod / 2], wlo[kMaxMod / 2];
 };
 
 /* --------------------------------------------------------------------------- preprocessing */
@@ -339,10 +344,18 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
   if (t >= (long long)M * N) return;
   const int j = (int)(t / M), i = (int)(t - (long long)j * M);
   const size_t plane = (size_t)M * N, off = (size_t)j * M + i;
-  /* s = frac(sum_q r_q * w_q), kept in [0, 1) as a double-double */
+  /* s = frac(sum_p r_p * w_p) over the moduli pairs, kept in [0, 1) as a double-double; r_p is the
+     residue modulo the pair's product (Garner's step: r_a + m_a ((r_b - r_a) m_a^-1 mod m_b)) */
   double sh = 0.0, sl = 0.0;
-  for (int q = 0; q < cs.nmod; ++q) {
-    const double r = (double)R[(size_t)q * plane + off];
+  for (int q = 0; q < cs.npair; ++q) {
+    const unsigned ra = R[(size_t)(2 * q) * plane + off];
+    unsigned rab = ra;
+    if (1u != cs.pb[q]) {
+      const unsigned mb = cs.pb[q], rb = R[(size_t)(2 * q + 1) * plane + off];
+      const unsigned ram = (ra >= mb) ? ra - mb : ra; /* ra < 256 < 2 mb */
+      rab = ra + cs.pa[q] * mod_small((unsigned long long)(rb + mb - ram) * cs.pinv[q], mb, cs.pbinv64[q]);
+    }
+    const double r = (double)rab;
     const double p = r * cs.whi[q];
     const double pe = fma(r, cs.whi[q], -p) + r * cs.wlo[q];
     double s, e;
@@ -351,13 +364,15 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
     sh = s + e;
     sl = e - (sh - s);
     const double f = floor(sh);
-    sh -= f; /* exact: sh < 2^10 */
+    sh -= f; /* exact: sh < 2^17 */
     two_sum(sh, sl, s, e);
     sh = s;
     sl = e;
   }
-  if (sh + sl < 0.0) sh += 1.0;
-  if (sh + sl >= 0.5) sh -= 1.0; /* centre: x in [-P/2, P/2) */
+  /* centre: x in [-P/2, P/2). sh is in [-1, 1) here and the shift by 1 only applies when |sh| >= 1/2,
+     where it is exact (Sterbenz); adding 1 to a small negative sh would round its low bits away */
+  if (sh + sl >= 0.5) sh -= 1.0;
+  else if (sh + sl < -0.5) sh += 1.0;
   const double x = fma(sh, cs.phi, fma(sh, cs.plo, sl * cs.phi));
   const int ia = ea[i], ib = eb[j];
   double v = 0.0;
@@ -455,15 +470,24 @@ int make_consts(int nmod, int K, Oz2Consts* cs) {
   }
   for (int i = 0; i < nmod; ++i) {
     const unsigned m = kModuli[i];
-    unsigned pm = 1; /* (P / m) mod m */
-    for (int j = 0; j < nmod; ++j) {
-      if (j != i) pm = (unsigned)(((unsigned long long)pm * (kModuli[j] % m)) % m);
-    }
-    const unsigned y = inv_mod(pm, m);
     cs->mod[i] = m;
     cs->inv64[i] = (256u == m) ? 0ull : (unsigned long long)(((unsigned __int128)1 << 64) / m) + 1ull;
-    cs->whi[i] = (double)y / (double)m;
-    cs->wlo[i] = fma(-cs->whi[i], (double)m, (double)y) / (double)m; /* the remainder y - whi*m is exact */
+  }
+  cs->npair = (nmod + 1) / 2;
+  for (int q = 0; q < cs->npair; ++q) {
+    const unsigned ma = kModuli[2 * q], mbq = (2 * q + 1 < nmod) ? kModuli[2 * q + 1] : 1u;
+    const unsigned long long mm = (unsigned long long)ma * mbq;
+    unsigned long long pm = 1; /* (P / (ma mb)) mod (ma mb) */
+    for (int j = 0; j < nmod; ++j) {
+      if (j != 2 * q && j != 2 * q + 1) pm = (pm * (kModuli[j] % mm)) % mm;
+    }
+    const unsigned y = inv_mod((unsigned)pm, (unsigned)mm);
+    cs->pa[q] = ma;
+    cs->pb[q] = mbq;
+    cs->pinv[q] = (1u != mbq) ? inv_mod(ma % mbq, mbq) : 0u;
+    cs->pbinv64[q] = (1u != mbq) ? (unsigned long long)(((unsigned __int128)1 << 64) / mbq) + 1ull : 0ull;
+    cs->whi[q] = (double)y / (double)mm;
+    cs->wlo[q] = fma(-cs->whi[q], (double)mm, (double)y) / (double)mm; /* the remainder y - whi*mm is exact */
   }
   int lgk = 0;
   while ((1ll << lgk) < (long long)K) ++lgk;

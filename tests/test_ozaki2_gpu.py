@@ -113,3 +113,19 @@ def test_large_square(acc):
     b = g.uniform(-1, 1, size=(N, N))
     got = run(A, stream, "N", "N", N, N, N, a, b, np.zeros((N, N)))
     assert relerr(got, a @ b) <= FP64_TOL
+
+
+def test_near_cancellation(acc):
+    """Outputs many orders of magnitude below |A| |B| (pairs of products that nearly cancel): the
+    reconstruction keeps its double-double precision whatever the sign of the small result."""
+    A, stream = acc
+    M, N, K = 64, 256, 64
+    g = W.rng(12)
+    a = g.uniform(-1, 1, size=(M, K))
+    a[:, 1::2] = a[:, 0::2]
+    b = g.uniform(-1, 1, size=(K, N))
+    b[1::2] = -b[0::2] * (1.0 + g.uniform(-1e-6, 1e-6, size=(K // 2, N)))
+    got = run(A, stream, "N", "N", M, N, K, a, b, np.zeros((M, N)))
+    ref = O.ozaki2_gemm(a, b, O.default_moduli(K))
+    assert np.max(np.abs(ref)) < 1e-4
+    assert relerr(got, ref) <= RECON_TOL
