@@ -335,15 +335,16 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
   e = (a - (s - bb)) + (b - bb);
 }
 
-/* C(i,j) = alpha * x * 2^E + beta * C(i,j), x the centred integer with residues R[.][j][i]. One
-   thread per element, consecutive threads on consecutive rows. */
+/* C(i,j) = alpha * x * 2^E + beta * C(i,j), x the centred integer with residues R[.][j][i]. Threads
+   over rows i, grid rows over columns j (strided when N exceeds the grid). */
 __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* __restrict__ R, int M, int N,
   const int* __restrict__ ea, const int* __restrict__ eb, const __grid_constant__ Oz2Consts cs, double alpha, double beta,
   double* __restrict__ C, long long ldc) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)M * N) return;
-  const int j = (int)(t / M), i = (int)(t - (long long)j * M);
-  const size_t plane = (size_t)M * N, off = (size_t)j * M + i;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const size_t plane = (size_t)M * N;
+  for (int j = blockIdx.y; j < N; j += gridDim.y) {
+  const size_t off = (size_t)j * M + i;
   /* s = frac(sum_p r_p * w_p) over the moduli pairs, kept in [0, 1) as a double-double; r_p is the
      residue modulo the pair's product (Garner's step: r_a + m_a ((r_b - r_a) m_a^-1 mod m_b)) */
   double sh = 0.0, sl = 0.0;
@@ -376,9 +377,13 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
   const double x = fma(sh, cs.phi, fma(sh, cs.plo, sl * cs.phi));
   const int ia = ea[i], ib = eb[j];
   double v = 0.0;
-  if (0 != ia && 0 != ib) v = ldexp(x, ia + ib - 2150 + 2 * (53 - cs.mb));
+  if (0 != ia && 0 != ib) {
+    const int E = ia + ib - 2150 + 2 * (53 - cs.mb);
+    v = (E >= -1022 && E <= 1023) ? x * __longlong_as_double((long long)(E + 1023) << 52) /* exact */ : ldexp(x, E);
+  }
   double* const cp = C + i + (long long)j * ldc;
   *cp = (0.0 == beta) ? alpha * v : fma(alpha, v, beta * *cp);
+  }
 }
 
 /* ------------------------------------------------------------------------------------ host */
@@ -607,7 +612,8 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
   }
   prof = xs_profile_begin(stream);
   const long long n = (long long)M * N;
-  xs_oz2_reconstruct<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rC, M, N, ea, eb, cs, alpha, beta, c, ldc);
+  xs_oz2_reconstruct<<<dim3((unsigned)((M + 255) / 256), (unsigned)(N < 65535 ? N : 65535)), 256, 0, s>>>(rC, M, N, ea, eb, cs,
+    alpha, beta, c, ldc);
   r = (int)cudaGetLastError();
   xs_profile_end(prof, "ozaki2_reconstruct", 0.0, (double)nmod * n + 16.0 * n, stream);
   return r;
