@@ -21,12 +21,13 @@
  * Device layout: residue planes rA[q][M][Kp] and rB[q][N][Kp] (u8, K contiguous, zero padded),
  * exponents ea[M], eb[N], residues of C R[q][N][M] (u8, column-major per modulus).
  *
- * GEMM kernel: one CTA per 128 x 256 tile of C, 6 warps, the pipeline of the scheme-1 kernel with
- * one accumulation group per modulus: warp 0 streams (modulus, k-block) tiles of both operands into
- * a 4-stage shared-memory ring with TMA (128-byte swizzle); warp 1 owns two 128 x 256 int32
- * accumulators in tensor memory and one lane issues the MMAs; warps 2-5 reduce a finished
- * accumulator modulo m_i and store the bytes while the tensor cores work on the next modulus. Every
- * mbarrier wait is bounded (per-call abort word, library device error word).
+ * GEMM kernel: persistent, one CTA per SM, 6 warps, the pipeline of the scheme-1 kernel over work
+ * units (modulus, 128 x 256 tile of C) taken modulus-major and strided by the grid: warp 0 streams
+ * the k-blocks of both operands' residue planes into a 4-stage shared-memory ring with TMA (128-byte
+ * swizzle); warp 1 owns two 128 x 256 int32 accumulators in tensor memory and one lane issues the
+ * MMAs; warps 2-5 reduce a finished accumulator modulo m_i and store the bytes while the tensor cores
+ * work on the next unit. Every mbarrier wait is bounded (per-call abort word, library device error
+ * word).
  */
 #include "internal.h"
 #include "tc_ptx.cuh"
@@ -58,14 +59,16 @@ constexpr unsigned kModuli[kMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 2
 
 struct Oz2Consts {
   unsigned mod[kMaxMod];
-  unsigned long long inv64[kMaxMod]; /* floor(2^64 / m_i) + 1: floor(u / m_i) = umulhi64(u, inv64) for u < 2^53 */
+  /* 32-bit residues (mod31): magic = floor(2^39 / m_i) + 1; c18 = 2^18 mod m_i, c36 = 2^36 mod m_i;
+     km = the least multiple of m_i that is at least 2^27 */
+  unsigned magic[kMaxMod], c18[kMaxMod], c36[kMaxMod], km[kMaxMod];
   double phi, plo; /* P as a double-double */
   int nmod, mb;
   /* reconstruction over moduli pairs (m_2p, m_2p+1), combined first into one residue modulo their
      product (a last unpaired modulus has pb = 1): pinv = m_2p^-1 mod m_2p+1, w = y / (m_2p m_2p+1) */
   int npair;
   unsigned pa[kMaxMod / 2], pb[kMaxMod / 2], pinv[kMaxMod / 2];
-  unsigned long long pbinv64[kMaxMod / 2];
+  unsigned pbmagic[kMaxMod / 2]; /* floor(2^39 / pb) + 1 */
   double whi[kMaxMod / 2], wlo[kMaxMod / 2];
 };
 
@@ -103,33 +106,40 @@ __device__ __forceinline__ unsigned long long aligned_int(double v, int erow, in
   return (0 != mt && sh < 64) ? (mt >> sh) : 0ull;
 }
 
-/* u mod m for u < 2^53 and m <= 256 from inv = floor(2^64 / m) + 1: the high product is
-   u/m + u*e/2^64 with 0 < e < 1, and since u/m is at most (m-1)/m <= 1 - 2^-8 above an integer
-   and u*e/2^64 < 2^-11, its integer part is floor(u / m) exactly. */
-__device__ __forceinline__ unsigned mod_small(unsigned long long u, unsigned m, unsigned long long inv) {
-  return (unsigned)(u - __umul64hi(u, inv) * m);
+
+/* x mod m for x < 2^31 and m <= 256 from magic = floor(2^39 / m) + 1 (< 2^32 for m >= 129): the
+   product x * magic / 2^39 is x/m + x*e/2^39 with 0 < e <= 1, x*e/2^39 < 2^-8 <= 1/m, and x/m is at
+   most 1 - 1/m above an integer, so the shifted high product is floor(x / m) exactly. */
+__device__ __forceinline__ unsigned mod31(unsigned x, unsigned m, unsigned magic) {
+  return x - (__umulhi(x, magic) >> 7) * m;
 }
 
-/* Residue of the signed integer (-1)^sign * u (u < 2^53) modulo m, in [0, m). */
-__device__ __forceinline__ unsigned residue(unsigned long long u, unsigned sign, unsigned m, unsigned long long inv) {
-  const unsigned x = (256u == m) ? ((unsigned)u & 255u) : mod_small(u, m, inv);
-  return (sign && 0u != x) ? m - x : x;
-}
-
-/* Residues of 16 consecutive k of one row into the planes d[i][r][k0 .. k0+15]. */
+/* Residues of 16 consecutive k of one row into the planes d[i][r][k0 .. k0+15]. Each integer
+   u < 2^53 is held as 18-bit limbs a0 + a1 2^18 + a2 2^36, so u = x (mod m) with
+   x = a0 + a1 c18 + a2 c36 < 2^27 (c = 2^18, 2^36 mod m), and -u = km - x (mod m) with km >= 2^27
+   a multiple of m: all 32-bit arithmetic. */
 __device__ __forceinline__ void residues16(const double (&v)[16], int erow, const Oz2Consts& cs, unsigned char* __restrict__ d,
   long long plane, long long off) {
-  unsigned long long u[16];
-  unsigned sg[16];
+  unsigned a0[16], a1[16], a2[16], sg[16];
 #pragma unroll
-  for (int j = 0; j < 16; ++j) u[j] = aligned_int(v[j], erow, cs.mb, sg[j]);
+  for (int j = 0; j < 16; ++j) {
+    const unsigned long long u = aligned_int(v[j], erow, cs.mb, sg[j]);
+    a0[j] = (unsigned)u & 0x3ffffu;
+    a1[j] = (unsigned)(u >> 18) & 0x3ffffu;
+    a2[j] = (unsigned)(u >> 36);
+  }
   for (int i = 0; i < cs.nmod; ++i) {
+    const unsigned m = cs.mod[i], mg = cs.magic[i], c1 = cs.c18[i], c2 = cs.c36[i], km = cs.km[i];
     uint32_t w[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       uint32_t x = 0;
 #pragma unroll
-      for (int b = 0; b < 4; ++b) x |= residue(u[q * 4 + b], sg[q * 4 + b], cs.mod[i], cs.inv64[i]) << (8 * b);
+      for (int b = 0; b < 4; ++b) {
+        const int j = q * 4 + b;
+        const unsigned t = a0[j] + a1[j] * c1 + a2[j] * c2;
+        x |= mod31(sg[j] ? km - t : t, m, mg) << (8 * b);
+      }
       w[q] = x;
     }
     *reinterpret_cast<uint4*>(d + i * plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -178,7 +188,7 @@ struct Oz2GemmArgs {
   int nmod;
   int first; /* 1: the first k-chunk (residues are written, not accumulated) */
   unsigned mod[kMaxMod];
-  unsigned long long inv64[kMaxMod];
+  unsigned magic[kMaxMod]; /* floor(2^39 / m_i) + 1 */
   unsigned char* R; /* [nmod][N][M] */
   unsigned* abort;
   unsigned* dev_err;
@@ -191,6 +201,17 @@ constexpr size_t gemm_smem_bytes() {
 /* instruction descriptor of tcgen05.mma kind::i8 with unsigned 8-bit A and B, s32 accumulator */
 __host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {
   return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+/* Work unit u of the persistent GEMM: modulus q = u / ntiles (modulus-major, so the CTAs resident at
+   one time read the residue planes of one or two moduli and those stay in L2), C tile by grouped
+   rasterization (kGroupM row panels sweep the column panels together). */
+__device__ __forceinline__ void unit_coords(int u, int ntiles, int ntm, int ntn, int& q, int& m0, int& n0) {
+  q = u / ntiles;
+  const int id = u - q * ntiles, per_group = kGroupM * ntn, g = id / per_group, first = g * kGroupM;
+  const int gsize = min(kGroupM, ntm - first), r = id - g * per_group;
+  m0 = (first + r % gsize) * kBM;
+  n0 = (r / gsize) * kBN;
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
@@ -209,14 +230,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned* const abort = args.abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int n0, m0; /* grouped rasterization: kGroupM row panels sweep the column panels together */
-  {
-    const int ntm = (args.M + kBM - 1) / kBM, ntn = (args.N + kBN - 1) / kBN;
-    const int id = blockIdx.x, per_group = kGroupM * ntn, g = id / per_group, first = g * kGroupM;
-    const int gsize = min(kGroupM, ntm - first), r = id - g * per_group;
-    m0 = (first + r % gsize) * kBM;
-    n0 = (r / gsize) * kBN;
-  }
+  const int ntm = (args.M + kBM - 1) / kBM, ntn = (args.N + kBN - 1) / kBN, ntiles = ntm * ntn;
+  const int nunits = ntiles * args.nmod;
   if (0 == threadIdx.x) {
     for (int i = 0; i < kStages; ++i) {
       mbar_init(&full[i], 1);
@@ -243,7 +258,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (0 == lane) {
       int it = 0;
       bool ok = true;
-      for (int q = 0; q < args.nmod && ok; ++q) {
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        int q, m0, n0;
+        unit_coords(u, ntiles, ntm, ntn, q, m0, n0);
         for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
           const int stage = it % kStages;
           const uint32_t ph = (uint32_t)(it / kStages) & 1u;
@@ -260,8 +277,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t idesc = idesc_u8(kBM, kBN);
       int it = 0;
       bool ok = true;
-      for (int q = 0; q < args.nmod && ok; ++q) {
-        const int buf = q & 1, use = q >> 1;
+      for (int u = blockIdx.x, i = 0; u < nunits && ok; u += gridDim.x, ++i) {
+        const int buf = i & 1, use = i >> 1;
         if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u))) break;
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(buf * kBN);
@@ -285,14 +302,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; thread = one row of the tile */
     const int qd = warp & 3;
-    const int row = m0 + qd * 32 + lane;
-    const bool rok = row < args.M;
-    for (int q = 0; q < args.nmod; ++q) {
-      const int buf = q & 1, use = q >> 1;
+    for (int u = blockIdx.x, i = 0; u < nunits; u += gridDim.x, ++i) {
+      const int buf = i & 1, use = i >> 1;
+      int q, m0, n0;
+      unit_coords(u, ntiles, ntm, ntn, q, m0, n0);
+      const int row = m0 + qd * 32 + lane;
+      const bool rok = row < args.M;
       if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u)) break;
       tc_fence_after();
       const unsigned m = args.mod[q];
-      const unsigned long long inv = args.inv64[q];
+      const unsigned mg = args.magic[q];
       unsigned char* const plane = args.R + (size_t)q * args.M * args.N;
       for (int c0 = 0; c0 < kBN; c0 += 32) {
         uint32_t v[32];
@@ -306,7 +325,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int j = 0; j < 32; ++j) prev[j] = (j < ncol && !args.first) ? dst[(size_t)j * args.M] : 0u;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
-            if (j < ncol) dst[(size_t)j * args.M] = (unsigned char)mod_small((unsigned long long)v[j] + prev[j], m, inv);
+            if (j < ncol) dst[(size_t)j * args.M] = (unsigned char)mod31(v[j] + prev[j], m, mg); /* < 2^31 */
           }
         }
       }
@@ -354,21 +373,17 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
     if (1u != cs.pb[q]) {
       const unsigned mb = cs.pb[q], rb = R[(size_t)(2 * q + 1) * plane + off];
       const unsigned ram = (ra >= mb) ? ra - mb : ra; /* ra < 256 < 2 mb */
-      rab = ra + cs.pa[q] * mod_small((unsigned long long)(rb + mb - ram) * cs.pinv[q], mb, cs.pbinv64[q]);
+      rab = ra + cs.pa[q] * mod31((rb + mb - ram) * cs.pinv[q], mb, cs.pbmagic[q]); /* < 2^17 */
     }
-    const double r = (double)rab;
+    const double r = __hiloint2double(0x43300000, (int)rab) - 0x1p52; /* exact conversion, rab < 2^17 */
     const double p = r * cs.whi[q];
-    const double pe = fma(r, cs.whi[q], -p) + r * cs.wlo[q];
+    const double pe = fma(r, cs.wlo[q], fma(r, cs.whi[q], -p));
     double s, e;
     two_sum(sh, p, s, e);
     e += sl + pe;
-    sh = s + e;
+    s -= (s + 0x1.8p52) - 0x1.8p52; /* drop the nearest integer (|s| < 2^18): exact, s in [-1/2, 1/2] */
+    sh = s + e;                     /* |e| < 2^-30: fast two-sum */
     sl = e - (sh - s);
-    const double f = floor(sh);
-    sh -= f; /* exact: sh < 2^17 */
-    two_sum(sh, sl, s, e);
-    sh = s;
-    sl = e;
   }
   /* centre: x in [-P/2, P/2). sh is in [-1, 1) here and the shift by 1 only applies when |sh| >= 1/2,
      where it is exact (Sterbenz); adding 1 to a small negative sh would round its low bits away */
@@ -476,7 +491,10 @@ int make_consts(int nmod, int K, Oz2Consts* cs) {
   for (int i = 0; i < nmod; ++i) {
     const unsigned m = kModuli[i];
     cs->mod[i] = m;
-    cs->inv64[i] = (256u == m) ? 0ull : (unsigned long long)(((unsigned __int128)1 << 64) / m) + 1ull;
+    cs->magic[i] = (unsigned)((1ull << 39) / m + 1ull);
+    cs->c18[i] = (unsigned)((1ull << 18) % m);
+    cs->c36[i] = (unsigned)((1ull << 36) % m);
+    cs->km[i] = (unsigned)(((1ull << 27) + m - 1) / m * m);
   }
   cs->npair = (nmod + 1) / 2;
   for (int q = 0; q < cs->npair; ++q) {
@@ -490,7 +508,7 @@ int make_consts(int nmod, int K, Oz2Consts* cs) {
     cs->pa[q] = ma;
     cs->pb[q] = mbq;
     cs->pinv[q] = (1u != mbq) ? inv_mod(ma % mbq, mbq) : 0u;
-    cs->pbinv64[q] = (1u != mbq) ? (unsigned long long)(((unsigned __int128)1 << 64) / mbq) + 1ull : 0ull;
+    cs->pbmagic[q] = (1u != mbq) ? (unsigned)((1ull << 39) / mbq + 1ull) : 0u;
     cs->whi[q] = (double)y / (double)mm;
     cs->wlo[q] = fma(-cs->whi[q], (double)mm, (double)y) / (double)mm; /* the remainder y - whi*mm is exact */
   }
@@ -586,7 +604,7 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
   args.nmod = nmod;
   for (int i = 0; i < nmod; ++i) {
     args.mod[i] = cs.mod[i];
-    args.inv64[i] = cs.inv64[i];
+    args.magic[i] = cs.magic[i];
   }
   args.R = rC;
   args.abort = abort;
@@ -599,7 +617,8 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
     smem_set = 1;
   }
   const int nkb = (K + kBK - 1) / kBK;
-  const dim3 grid(((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM));
+  const long long nunits = (long long)((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM) * nmod;
+  const dim3 grid((unsigned)(nunits < xs_sm_count() ? nunits : xs_sm_count()));
   for (int kb0 = 0; kb0 < nkb; kb0 += kKChunkBlocks) {
     args.kb0 = kb0;
     args.kb1 = (kb0 + kKChunkBlocks < nkb) ? kb0 + kKChunkBlocks : nkb;
