@@ -12,8 +12,10 @@
  * epilogue and kept as one byte per modulus and output), and the integer is reconstructed from its
  * residues by the CRT with the "fractional" formula
  *     x / P = frac( sum_i r_i * y_i / m_i ),   P = prod m_i,  y_i = (P / m_i)^-1 mod m_i,
- * evaluated in double-double arithmetic (Dekker's two-product with an FMA and Knuth's two-sum),
- * centred to [-P/2, P/2) and scaled back: C(i,j) = x * 2^(ea_i + eb_j - 2150 + 2 (53 - MB)).
+ * evaluated as a 128-bit binary fraction in integer arithmetic (y_i / m_i rounded to 2^-128; the sum
+ * wraps modulo 2^128, which takes the fractional part, and read as a signed number it is centred:
+ * x in [-P/2, P/2)), multiplied by P in double precision and scaled back:
+ * C(i,j) = x * 2^(ea_i + eb_j - 2150 + 2 (53 - MB)).
  * The modulus count decides the precision: P must exceed 2 K 2^(2 MB), so q moduli carry
  * MB = floor((log2 P - ceil(log2 K) - 2) / 2) bits per input (capped at 53); the default takes the fewest
  * moduli that give MB = 53 for this K (16 up to K = 2^17).
@@ -64,12 +66,9 @@ struct Oz2Consts {
   unsigned magic[kMaxMod], c18[kMaxMod], c36[kMaxMod], km[kMaxMod];
   double phi, plo; /* P as a double-double */
   int nmod, mb;
-  /* reconstruction over moduli pairs (m_2p, m_2p+1), combined first into one residue modulo their
-     product (a last unpaired modulus has pb = 1): pinv = m_2p^-1 mod m_2p+1, w = y / (m_2p m_2p+1) */
-  int npair;
-  unsigned pa[kMaxMod / 2], pb[kMaxMod / 2], pinv[kMaxMod / 2];
-  unsigned pbmagic[kMaxMod / 2]; /* floor(2^39 / pb) + 1 */
-  double whi[kMaxMod / 2], wlo[kMaxMod / 2];
+  /* w_i = y_i / m_i as a 128-bit binary fraction (floor(2^128 y_i / m_i)), least significant word
+     first; y_i = (P / m_i)^-1 mod m_i */
+  unsigned w[kMaxMod][4];
 };
 
 /* --------------------------------------------------------------------------- preprocessing */
@@ -114,36 +113,39 @@ __device__ __forceinline__ unsigned mod31(unsigned x, unsigned m, unsigned magic
   return x - (__umulhi(x, magic) >> 7) * m;
 }
 
-/* Residues of 16 consecutive k of one row into the planes d[i][r][k0 .. k0+15]. Each integer
-   u < 2^53 is held as 18-bit limbs a0 + a1 2^18 + a2 2^36, so u = x (mod m) with
-   x = a0 + a1 c18 + a2 c36 < 2^27 (c = 2^18, 2^36 mod m), and -u = km - x (mod m) with km >= 2^27
-   a multiple of m: all 32-bit arithmetic. */
-__device__ __forceinline__ void residues16(const double (&v)[16], int erow, const Oz2Consts& cs, unsigned char* __restrict__ d,
-  long long plane, long long off) {
+/* 16 consecutive k of one row as signed integers: each u < 2^53 is held as 18-bit limbs
+   a0 + a1 2^18 + a2 2^36, so u = x (mod m) with x = a0 + a1 c18 + a2 c36 < 2^27 (c = 2^18, 2^36 mod m),
+   and -u = km - x (mod m) with km >= 2^27 a multiple of m: all 32-bit arithmetic. */
+struct Limbs16 {
   unsigned a0[16], a1[16], a2[16], sg[16];
+};
+
+__device__ __forceinline__ void limbs16(const double (&v)[16], int erow, int mb, Limbs16& L) {
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    const unsigned long long u = aligned_int(v[j], erow, cs.mb, sg[j]);
-    a0[j] = (unsigned)u & 0x3ffffu;
-    a1[j] = (unsigned)(u >> 18) & 0x3ffffu;
-    a2[j] = (unsigned)(u >> 36);
+    const unsigned long long u = aligned_int(v[j], erow, mb, L.sg[j]);
+    L.a0[j] = (unsigned)u & 0x3ffffu;
+    L.a1[j] = (unsigned)(u >> 18) & 0x3ffffu;
+    L.a2[j] = (unsigned)(u >> 36);
   }
-  for (int i = 0; i < cs.nmod; ++i) {
-    const unsigned m = cs.mod[i], mg = cs.magic[i], c1 = cs.c18[i], c2 = cs.c36[i], km = cs.km[i];
-    uint32_t w[4];
+}
+
+/* The 16 residues modulo m_i as bytes (k ascending). */
+__device__ __forceinline__ uint4 residue_bytes16(const Limbs16& L, const Oz2Consts& cs, int i) {
+  const unsigned m = cs.mod[i], mg = cs.magic[i], c1 = cs.c18[i], c2 = cs.c36[i], km = cs.km[i];
+  uint32_t w[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint32_t x = 0;
+  for (int q = 0; q < 4; ++q) {
+    uint32_t x = 0;
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int j = q * 4 + b;
-        const unsigned t = a0[j] + a1[j] * c1 + a2[j] * c2;
-        x |= mod31(sg[j] ? km - t : t, m, mg) << (8 * b);
-      }
-      w[q] = x;
+    for (int b = 0; b < 4; ++b) {
+      const int j = q * 4 + b;
+      const unsigned t = L.a0[j] + L.a1[j] * c1 + L.a2[j] * c2;
+      x |= mod31(L.sg[j] ? km - t : t, m, mg) << (8 * b);
     }
-    *reinterpret_cast<uint4*>(d + i * plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
+    w[q] = x;
   }
+  return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 /* k contiguous (element (r, k) at x[k + r*ld]): one thread per (row, 16 k). */
@@ -157,19 +159,47 @@ __global__ void xs_oz2_res_kc(const double* __restrict__ x, long long ld, int R,
   double v[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? row[k0 + j] : 0.0;
-  residues16(v, emax[r], cs, d, (long long)R * Kp, (long long)r * Kp + k0);
+  Limbs16 L;
+  limbs16(v, emax[r], cs.mb, L);
+  unsigned char* const dst = d + (long long)r * Kp + k0;
+  const long long plane = (long long)R * Kp;
+  for (int i = 0; i < cs.nmod; ++i) *reinterpret_cast<uint4*>(dst + i * plane) = residue_bytes16(L, cs, i);
 }
 
-/* rows contiguous (element (r, k) at x[r + k*ld]): threads over rows, blockIdx.y over 16 k. */
-__global__ void xs_oz2_res_rc(const double* __restrict__ x, long long ld, int R, int K, int Kp, const int* __restrict__ emax,
-  const __grid_constant__ Oz2Consts cs, unsigned char* __restrict__ d) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= R) return;
-  const int k0 = blockIdx.y * 16;
+/* rows contiguous (element (r, k) at x[r + k*ld]): a block of 256 threads takes 32 rows x 128 k,
+   lane = row (coalesced loads), warp = 16 k. The residue bytes of four moduli at a time go through
+   shared memory (rows padded to 144 bytes: the 16-byte chunks of 8 lanes fall in distinct banks) and
+   leave as whole 128-byte row segments of each plane, so no 32-byte sector is written in part. */
+constexpr int kRcRows = 32, kRcK = 128, kRcPitch = kRcK + 16, kRcMods = 4;
+__global__ void __launch_bounds__(256) xs_oz2_res_rc(const double* __restrict__ x, long long ld, int R, int K, int Kp,
+  const int* __restrict__ emax, const __grid_constant__ Oz2Consts cs, unsigned char* __restrict__ d) {
+  __shared__ __align__(16) unsigned char tile[kRcMods][kRcRows * kRcPitch];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r0 = blockIdx.x * kRcRows, kt0 = blockIdx.y * kRcK;
+  const int r = r0 + lane, k0 = kt0 + warp * 16;
   double v[16];
 #pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? x[r + (long long)(k0 + j) * ld] : 0.0;
-  residues16(v, emax[r], cs, d, (long long)R * Kp, (long long)r * Kp + k0);
+  for (int j = 0; j < 16; ++j) v[j] = (r < R && k0 + j < K) ? x[r + (long long)(k0 + j) * ld] : 0.0;
+  Limbs16 L;
+  limbs16(v, (r < R) ? emax[r] : 0, cs.mb, L);
+  const long long plane = (long long)R * Kp;
+  /* write-out role: row wr of the tile, 16-byte chunk wc */
+  const int wr = threadIdx.x >> 3, wc = threadIdx.x & 7;
+  const bool wok = (r0 + wr < R) && (kt0 + wc * 16 < Kp);
+  unsigned char* const dst = d + (long long)(r0 + wr) * Kp + kt0 + wc * 16;
+  for (int i0 = 0; i0 < cs.nmod; i0 += kRcMods) {
+    const int nm = min(kRcMods, cs.nmod - i0);
+    for (int ii = 0; ii < nm; ++ii) {
+      *reinterpret_cast<uint4*>(&tile[ii][lane * kRcPitch + warp * 16]) = residue_bytes16(L, cs, i0 + ii);
+    }
+    __syncthreads();
+    if (wok) {
+      for (int ii = 0; ii < nm; ++ii) {
+        *reinterpret_cast<uint4*>(dst + (i0 + ii) * plane) = *reinterpret_cast<const uint4*>(&tile[ii][wr * kRcPitch + wc * 16]);
+      }
+    }
+    __syncthreads();
+  }
 }
 
 /* C = beta * C (K == 0 or alpha == 0). */
@@ -347,57 +377,71 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 /* ---------------------------------------------------------------------------- reconstruction */
 
-/* Knuth's two-sum and Dekker's two-product (with an FMA): s + e == a + b, p + e == a * b exactly. */
-__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-  s = a + b;
-  const double bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
+/* S += r * W (mod 2^128), S and W as four 32-bit words, least significant first. */
+__device__ __forceinline__ void mac128(uint32_t (&S)[4], uint32_t r, const unsigned (&W)[4]) {
+  asm("mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
+      "madc.lo.cc.u32 %1, %4, %6, %1;\n\t"
+      "madc.lo.cc.u32 %2, %4, %7, %2;\n\t"
+      "madc.lo.u32 %3, %4, %8, %3;\n\t"
+      "mad.hi.cc.u32 %1, %4, %5, %1;\n\t"
+      "madc.hi.cc.u32 %2, %4, %6, %2;\n\t"
+      "madc.hi.u32 %3, %4, %7, %3;"
+      : "+r"(S[0]), "+r"(S[1]), "+r"(S[2]), "+r"(S[3])
+      : "r"(r), "r"(W[0]), "r"(W[1]), "r"(W[2]), "r"(W[3]));
 }
 
-/* C(i,j) = alpha * x * 2^E + beta * C(i,j), x the centred integer with residues R[.][j][i]. Threads
-   over rows i, grid rows over columns j (strided when N exceeds the grid). */
+/* x * 2^E from the 128-bit fraction S of x / P (see xs_oz2_reconstruct). */
+__device__ __forceinline__ double crt_value(const uint32_t (&S)[4], const Oz2Consts& cs, int E) {
+  /* fraction = (T + U 2^-64) 2^-64, T the signed upper and U the unsigned lower 64 bits; T as a
+     double plus the (exact, |.| <= 2^10) rest of its rounding */
+  const long long T = (long long)(((unsigned long long)S[3] << 32) | S[2]);
+  const unsigned long long U = ((unsigned long long)S[1] << 32) | S[0];
+  const double th = __ll2double_rn(T);
+  const double tl = __ll2double_rn(T - __double2ll_rn(th)) + __ull2double_rn(U) * 0x1p-64;
+  const double x = fma(th, cs.phi, fma(th, cs.plo, tl * cs.phi)); /* x * 2^64 */
+  E -= 64;
+  return (E >= -1022 && E <= 1023) ? x * __longlong_as_double((long long)(E + 1023) << 52) /* exact */ : ldexp(x, E);
+}
+
+/* C(i,j) = alpha * x * 2^E + beta * C(i,j), x the centred integer with residues R[.][j][i]. A thread
+   takes V consecutive rows i (one V-byte load per plane; V = 4 needs M % 4 == 0), grid rows take
+   columns j (strided when N exceeds the grid).
+   x / P = frac(sum_i r_i w_i) is accumulated as a 128-bit binary fraction: the wrap-around modulo 2^128
+   takes the fractional part and the two's-complement reading of the sum centres it to [-1/2, 1/2)
+   (x in [-P/2, P/2)). With w_i rounded down to 2^-128 the fraction is off by less than
+   nmod * 255 * 2^-128 < 2^-115, i.e. x by less than 2^-115 P. */
+template <int V>
 __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* __restrict__ R, int M, int N,
   const int* __restrict__ ea, const int* __restrict__ eb, const __grid_constant__ Oz2Consts cs, double alpha, double beta,
   double* __restrict__ C, long long ldc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= M) return;
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+  if (i0 >= M) return;
   const size_t plane = (size_t)M * N;
+  int ia[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) ia[v] = (i0 + v < M) ? ea[i0 + v] : 0;
   for (int j = blockIdx.y; j < N; j += gridDim.y) {
-  const size_t off = (size_t)j * M + i;
-  /* s = frac(sum_p r_p * w_p) over the moduli pairs, kept in [0, 1) as a double-double; r_p is the
-     residue modulo the pair's product (Garner's step: r_a + m_a ((r_b - r_a) m_a^-1 mod m_b)) */
-  double sh = 0.0, sl = 0.0;
-  for (int q = 0; q < cs.npair; ++q) {
-    const unsigned ra = R[(size_t)(2 * q) * plane + off];
-    unsigned rab = ra;
-    if (1u != cs.pb[q]) {
-      const unsigned mb = cs.pb[q], rb = R[(size_t)(2 * q + 1) * plane + off];
-      const unsigned ram = (ra >= mb) ? ra - mb : ra; /* ra < 256 < 2 mb */
-      rab = ra + cs.pa[q] * mod31((rb + mb - ram) * cs.pinv[q], mb, cs.pbmagic[q]); /* < 2^17 */
+    const size_t off = (size_t)j * M + i0;
+    unsigned res[kMaxMod]; /* V residues per word, every load in flight before the arithmetic starts */
+#pragma unroll
+    for (int q = 0; q < kMaxMod; ++q) {
+      if (4 == V) res[q] = (q < cs.nmod) ? *reinterpret_cast<const unsigned*>(R + (size_t)q * plane + off) : 0u;
+      else res[q] = (q < cs.nmod) ? R[(size_t)q * plane + off] : 0u;
     }
-    const double r = __hiloint2double(0x43300000, (int)rab) - 0x1p52; /* exact conversion, rab < 2^17 */
-    const double p = r * cs.whi[q];
-    const double pe = fma(r, cs.wlo[q], fma(r, cs.whi[q], -p));
-    double s, e;
-    two_sum(sh, p, s, e);
-    e += sl + pe;
-    s -= (s + 0x1.8p52) - 0x1.8p52; /* drop the nearest integer (|s| < 2^18): exact, s in [-1/2, 1/2] */
-    sh = s + e;                     /* |e| < 2^-30: fast two-sum */
-    sl = e - (sh - s);
-  }
-  /* centre: x in [-P/2, P/2). sh is in [-1, 1) here and the shift by 1 only applies when |sh| >= 1/2,
-     where it is exact (Sterbenz); adding 1 to a small negative sh would round its low bits away */
-  if (sh + sl >= 0.5) sh -= 1.0;
-  else if (sh + sl < -0.5) sh += 1.0;
-  const double x = fma(sh, cs.phi, fma(sh, cs.plo, sl * cs.phi));
-  const int ia = ea[i], ib = eb[j];
-  double v = 0.0;
-  if (0 != ia && 0 != ib) {
-    const int E = ia + ib - 2150 + 2 * (53 - cs.mb);
-    v = (E >= -1022 && E <= 1023) ? x * __longlong_as_double((long long)(E + 1023) << 52) /* exact */ : ldexp(x, E);
-  }
-  double* const cp = C + i + (long long)j * ldc;
-  *cp = (0.0 == beta) ? alpha * v : fma(alpha, v, beta * *cp);
+    const int ib = eb[j];
+    double* const cp = C + i0 + (long long)j * ldc;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      uint32_t S[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int q = 0; q < kMaxMod; ++q) {
+        if (q < cs.nmod) mac128(S, (res[q] >> (8 * v)) & 255u, cs.w[q]);
+      }
+      if (i0 + v < M) {
+        const double val = (0 != ia[v] && 0 != ib) ? crt_value(S, cs, ia[v] + ib - 2150 + 2 * (53 - cs.mb)) : 0.0;
+        cp[v] = (0.0 == beta) ? alpha * val : fma(alpha, val, beta * cp[v]);
+      }
+    }
   }
 }
 
@@ -471,8 +515,8 @@ int make_consts(int nmod, int K, Oz2Consts* cs) {
       if (1u != gcd_host(kModuli[i], kModuli[j])) return 0;
     }
   }
-  /* P as a 128-bit integer (product of at most 20 factors <= 2^8 fits up to 16 factors exactly;
-     beyond that only the double-double value of P matters, computed by scaling) */
+  /* P as a double-double: exact from a 128-bit integer up to 16 factors <= 2^8, from a long double
+     beyond */
   unsigned __int128 P = 1;
   long double Pld = 1.0L;
   for (int i = 0; i < nmod; ++i) {
@@ -496,21 +540,18 @@ int make_consts(int nmod, int K, Oz2Consts* cs) {
     cs->c36[i] = (unsigned)((1ull << 36) % m);
     cs->km[i] = (unsigned)(((1ull << 27) + m - 1) / m * m);
   }
-  cs->npair = (nmod + 1) / 2;
-  for (int q = 0; q < cs->npair; ++q) {
-    const unsigned ma = kModuli[2 * q], mbq = (2 * q + 1 < nmod) ? kModuli[2 * q + 1] : 1u;
-    const unsigned long long mm = (unsigned long long)ma * mbq;
-    unsigned long long pm = 1; /* (P / (ma mb)) mod (ma mb) */
+  for (int i = 0; i < nmod; ++i) {
+    const unsigned m = kModuli[i];
+    unsigned pm = 1; /* (P / m_i) mod m_i */
     for (int j = 0; j < nmod; ++j) {
-      if (j != 2 * q && j != 2 * q + 1) pm = (pm * (kModuli[j] % mm)) % mm;
+      if (j != i) pm = (pm * (kModuli[j] % m)) % m;
     }
-    const unsigned y = inv_mod((unsigned)pm, (unsigned)mm);
-    cs->pa[q] = ma;
-    cs->pb[q] = mbq;
-    cs->pinv[q] = (1u != mbq) ? inv_mod(ma % mbq, mbq) : 0u;
-    cs->pbmagic[q] = (1u != mbq) ? (unsigned)((1ull << 39) / mbq + 1ull) : 0u;
-    cs->whi[q] = (double)y / (double)mm;
-    cs->wlo[q] = fma(-cs->whi[q], (double)mm, (double)y) / (double)mm; /* the remainder y - whi*mm is exact */
+    unsigned long long rem = inv_mod(pm, m); /* y_i < m_i: floor(2^128 y_i / m_i) by long division */
+    for (int k = 3; k >= 0; --k) {
+      const unsigned long long num = rem << 32;
+      cs->w[i][k] = (unsigned)(num / m);
+      rem = num % m;
+    }
   }
   int lgk = 0;
   while ((1ll << lgk) < (long long)K) ++lgk;
@@ -534,7 +575,7 @@ int residue_operand(const double* x, long long ld, bool rows_contiguous, int R, 
   if (rows_contiguous) {
     const int kchunk = 256;
     xs_oz2_rowexp_rc<<<dim3((R + 255) / 256, (K + kchunk - 1) / kchunk), 256, 0, s>>>(x, ld, R, K, kchunk, emax);
-    xs_oz2_res_rc<<<dim3((R + 127) / 128, Kp / 16), 128, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
+    xs_oz2_res_rc<<<dim3((R + kRcRows - 1) / kRcRows, (Kp + kRcK - 1) / kRcK), 256, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
   }
   else {
     xs_oz2_rowexp_kc<<<(R + 7) / 8, 256, 0, s>>>(x, ld, R, K, emax);
@@ -631,8 +672,10 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
   }
   prof = xs_profile_begin(stream);
   const long long n = (long long)M * N;
-  xs_oz2_reconstruct<<<dim3((unsigned)((M + 255) / 256), (unsigned)(N < 65535 ? N : 65535)), 256, 0, s>>>(rC, M, N, ea, eb, cs,
-    alpha, beta, c, ldc);
+  const int V = (0 == M % 4) ? 4 : 1;
+  const dim3 rgrid((unsigned)((M + 256 * V - 1) / (256 * V)), (unsigned)(N < 65535 ? N : 65535));
+  if (4 == V) xs_oz2_reconstruct<4><<<rgrid, 256, 0, s>>>(rC, M, N, ea, eb, cs, alpha, beta, c, ldc);
+  else xs_oz2_reconstruct<1><<<rgrid, 256, 0, s>>>(rC, M, N, ea, eb, cs, alpha, beta, c, ldc);
   r = (int)cudaGetLastError();
   xs_profile_end(prof, "ozaki2_reconstruct", 0.0, (double)nmod * n + 16.0 * n, stream);
   return r;
