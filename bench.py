@@ -290,36 +290,52 @@ def run_b200(args, d: Dist):
                                            ctypes.byref(gb)) == 0:
             prof[name] = {"launches": nl.value, "ms": ms.value, "gflop": gf.value, "gbyte": gb.value}
 
-    # end to end through the C-ABI with pinned host buffers
+    # end to end through the C-ABI with pinned host buffers. Two streams take alternate steps, each
+    # with its own device buffers (DBCSR drives several streams the same way), so the upload of one
+    # step overlaps the kernels and the download of the previous one; every step still copies its
+    # inputs in and its C out.
     e2e_steps = args.e2e_steps or min(args.steps, 50)
     ha = A.HostBuf(case.a.shape, np.float64, stream)
     hb = A.HostBuf(case.b.shape, np.float64, stream)
     hs = A.HostBuf(case.stack.shape, np.int32, stream)
-    hc = A.HostBuf((case.nc * m * n,), np.float64, stream)
     ha.array[:] = case.a
     hb.array[:] = case.b
     hs.array[:] = case.stack
-    e0, e1 = ctypes.c_void_p(), ctypes.c_void_p()
-    L.libxstream_b200_event_create_timed(ctypes.byref(e0))
-    L.libxstream_b200_event_create_timed(ctypes.byref(e1))
+    e2e_streams = [stream, A.Stream("bench-e2e")]
+    e2e_sets = []
+    for st in e2e_streams:
+        dc2 = A.DevBuf(case.nc * m * n * 8)
+        dc2.zero(st)
+        e2e_sets.append((A.DevBuf(case.a.nbytes), A.DevBuf(case.b.nbytes), A.DevBuf(case.stack.nbytes), dc2,
+                         A.HostBuf((case.nc * m * n,), np.float64, st)))
+    e0, e1, ej = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    for e in (e0, e1, ej):
+        L.libxstream_b200_event_create_timed(ctypes.byref(e))
 
-    def e2e_step():
-        xs.check(L.c_dbcsr_acc_memcpy_h2d(ha.ptr, da.ptr, case.a.nbytes, stream.handle), "h2d a")
-        xs.check(L.c_dbcsr_acc_memcpy_h2d(hb.ptr, db.ptr, case.b.nbytes, stream.handle), "h2d b")
-        xs.check(L.c_dbcsr_acc_memcpy_h2d(hs.ptr, ds.ptr, case.stack.nbytes, stream.handle), "h2d stack")
-        xs.check(A.transpose(trs, 0, case.nb, db, k, n, stream), "transpose")
-        xs.check(A.process(ds, S, da, db, dc, m, n, k, stream), "process")
-        xs.check(L.c_dbcsr_acc_memcpy_d2h(dc.ptr, hc.ptr, hc.array.nbytes, stream.handle), "d2h c")
+    def e2e_step(i):
+        st = e2e_streams[i % 2]
+        xa, xb, xsk, xc, hc = e2e_sets[i % 2]
+        xs.check(L.c_dbcsr_acc_memcpy_h2d(ha.ptr, xa.ptr, case.a.nbytes, st.handle), "h2d a")
+        xs.check(L.c_dbcsr_acc_memcpy_h2d(hb.ptr, xb.ptr, case.b.nbytes, st.handle), "h2d b")
+        xs.check(L.c_dbcsr_acc_memcpy_h2d(hs.ptr, xsk.ptr, case.stack.nbytes, st.handle), "h2d stack")
+        xs.check(A.transpose(trs, 0, case.nb, xb, k, n, st), "transpose")
+        xs.check(A.process(xsk, S, xa, xb, xc, m, n, k, st), "process")
+        xs.check(L.c_dbcsr_acc_memcpy_d2h(xc.ptr, hc.ptr, hc.array.nbytes, st.handle), "d2h c")
 
-    for _ in range(3):
-        e2e_step()
-    stream.sync()
+    for i in range(4):
+        e2e_step(i)
+    for st in e2e_streams:
+        st.sync()
     d.barrier()
     L.c_dbcsr_acc_event_record(e0.value, stream.handle)
-    for _ in range(e2e_steps):
-        e2e_step()
+    xs.check(L.c_dbcsr_acc_stream_wait_event(e2e_streams[1].handle, e0.value), "stream_wait_event")
+    for i in range(e2e_steps):
+        e2e_step(i)
+    L.c_dbcsr_acc_event_record(ej.value, e2e_streams[1].handle)
+    xs.check(L.c_dbcsr_acc_stream_wait_event(stream.handle, ej.value), "stream_wait_event")
     L.c_dbcsr_acc_event_record(e1.value, stream.handle)
-    stream.sync()
+    for st in e2e_streams:
+        st.sync()
     d.barrier()
     e2e_ms = d.max(L.libxstream_b200_event_elapsed_ms(e0.value, e1.value)) / e2e_steps
     e2e_value = d.world * case.flops / (e2e_ms * 1e-3) * 1e-9
@@ -367,12 +383,20 @@ def run_b200(args, d: Dist):
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(case.a.nbytes + case.b.nbytes + case.stack.nbytes),
-                    "d2h_bytes_per_step": int(hc.array.nbytes),
-                    "path": "h2d A,B,stack -> libsmm_acc_transpose(B) -> libsmm_acc_process -> d2h C"},
+                    "d2h_bytes_per_step": int(e2e_sets[0][4].array.nbytes),
+                    "path": "h2d A,B,stack -> libsmm_acc_transpose(B) -> libsmm_acc_process -> d2h C, "
+                            "two streams taking alternate steps"},
             "gpu_launches": kernels_per_step * args.steps, "kernels_per_step": kernels_per_step,
             "kernel_profile": prof, "clocks": clocks}
-    for b in (ha, hb, hs, hc):
+    for b in (ha, hb, hs):
         b.free(stream)
+    for xa, xb, xsk, xc, hc in e2e_sets:
+        hc.free(stream)
+        for b in (xa, xb, xsk, xc):
+            b.free()
+    e2e_streams[1].destroy()
+    for e in (e0, e1, ej):
+        L.c_dbcsr_acc_event_destroy(e.value)
     for b in (da, db, trs, dc, ds, flush):
         b.free()
     stream.destroy()

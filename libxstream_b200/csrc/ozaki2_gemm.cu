@@ -148,7 +148,9 @@ __device__ __forceinline__ uint4 residue_bytes16(const Limbs16& L, const Oz2Cons
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-/* k contiguous (element (r, k) at x[k + r*ld]): one thread per (row, 16 k). */
+/* k contiguous (element (r, k) at x[k + r*ld]): one thread per (row, 16 k); VEC: 16-byte loads
+   (x 16-byte aligned and ld even). */
+template <bool VEC>
 __global__ void xs_oz2_res_kc(const double* __restrict__ x, long long ld, int R, int K, int Kp, const int* __restrict__ emax,
   const __grid_constant__ Oz2Consts cs, unsigned char* __restrict__ d) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -157,8 +159,18 @@ __global__ void xs_oz2_res_kc(const double* __restrict__ x, long long ld, int R,
   const int r = (int)(t / kg), k0 = (int)(t - (long long)r * kg) * 16;
   const double* const row = x + (long long)r * ld;
   double v[16];
+  if (VEC && k0 + 16 <= K) {
 #pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? row[k0 + j] : 0.0;
+    for (int j = 0; j < 8; ++j) {
+      const double2 t2 = *reinterpret_cast<const double2*>(row + k0 + 2 * j);
+      v[2 * j] = t2.x;
+      v[2 * j + 1] = t2.y;
+    }
+  }
+  else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? row[k0 + j] : 0.0;
+  }
   Limbs16 L;
   limbs16(v, emax[r], cs.mb, L);
   unsigned char* const dst = d + (long long)r * Kp + k0;
@@ -377,19 +389,6 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 /* ---------------------------------------------------------------------------- reconstruction */
 
-/* S += r * W (mod 2^128), S and W as four 32-bit words, least significant first. */
-__device__ __forceinline__ void mac128(uint32_t (&S)[4], uint32_t r, const unsigned (&W)[4]) {
-  asm("mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
-      "madc.lo.cc.u32 %1, %4, %6, %1;\n\t"
-      "madc.lo.cc.u32 %2, %4, %7, %2;\n\t"
-      "madc.lo.u32 %3, %4, %8, %3;\n\t"
-      "mad.hi.cc.u32 %1, %4, %5, %1;\n\t"
-      "madc.hi.cc.u32 %2, %4, %6, %2;\n\t"
-      "madc.hi.u32 %3, %4, %7, %3;"
-      : "+r"(S[0]), "+r"(S[1]), "+r"(S[2]), "+r"(S[3])
-      : "r"(r), "r"(W[0]), "r"(W[1]), "r"(W[2]), "r"(W[3]));
-}
-
 /* x * 2^E from the 128-bit fraction S of x / P (see xs_oz2_reconstruct). */
 __device__ __forceinline__ double crt_value(const uint32_t (&S)[4], const Oz2Consts& cs, int E) {
   /* fraction = (T + U 2^-64) 2^-64, T the signed upper and U the unsigned lower 64 bits; T as a
@@ -406,7 +405,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&S)[4], const Oz2Con
 /* C(i,j) = alpha * x * 2^E + beta * C(i,j), x the centred integer with residues R[.][j][i]. A thread
    takes V consecutive rows i (one V-byte load per plane; V = 4 needs M % 4 == 0), grid rows take
    columns j (strided when N exceeds the grid).
-   x / P = frac(sum_i r_i w_i) is accumulated as a 128-bit binary fraction: the wrap-around modulo 2^128
+   x / P = frac(sum_i r_i w_i) is summed as a 128-bit binary fraction: the wrap-around modulo 2^128
    takes the fractional part and the two's-complement reading of the sum centres it to [-1/2, 1/2)
    (x in [-P/2, P/2)). With w_i rounded down to 2^-128 the fraction is off by less than
    nmod * 255 * 2^-128 < 2^-115, i.e. x by less than 2^-115 P. */
@@ -432,11 +431,26 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
     double* const cp = C + i0 + (long long)j * ldc;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      uint32_t S[4] = {0u, 0u, 0u, 0u};
+      /* sum_i r_i w_i column by column: word k of the product sums to < 20 * 2^8 * 2^32 < 2^45 in
+         64 bits, so no carry moves until the columns are combined (modulo 2^128) at the end */
+      unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
       for (int q = 0; q < kMaxMod; ++q) {
-        if (q < cs.nmod) mac128(S, (res[q] >> (8 * v)) & 255u, cs.w[q]);
+        if (q < cs.nmod) {
+          const unsigned r = (res[q] >> (8 * v)) & 255u;
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[w] += (unsigned long long)r * cs.w[q][w];
+        }
       }
+      uint32_t S[4];
+      unsigned long long t = acc[0];
+      S[0] = (uint32_t)t;
+      t = acc[1] + (t >> 32);
+      S[1] = (uint32_t)t;
+      t = acc[2] + (t >> 32);
+      S[2] = (uint32_t)t;
+      t = acc[3] + (t >> 32);
+      S[3] = (uint32_t)t;
       if (i0 + v < M) {
         const double val = (0 != ia[v] && 0 != ib) ? crt_value(S, cs, ia[v] + ib - 2150 + 2 * (53 - cs.mb)) : 0.0;
         cp[v] = (0.0 == beta) ? alpha * val : fma(alpha, val, beta * cp[v]);
@@ -580,7 +594,12 @@ int residue_operand(const double* x, long long ld, bool rows_contiguous, int R, 
   else {
     xs_oz2_rowexp_kc<<<(R + 7) / 8, 256, 0, s>>>(x, ld, R, K, emax);
     const long long n = (long long)R * (Kp / 16);
-    xs_oz2_res_kc<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
+    if (0 == ((uintptr_t)x & 15) && 0 == (ld & 1)) {
+      xs_oz2_res_kc<true><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
+    }
+    else {
+      xs_oz2_res_kc<false><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, ld, R, K, Kp, emax, cs, planes);
+    }
   }
   return (int)cudaGetLastError();
 }
