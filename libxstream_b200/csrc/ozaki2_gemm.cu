@@ -62,8 +62,8 @@ constexpr unsigned kModuli[kMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 2
 struct Oz2Consts {
   unsigned mod[kMaxMod];
   /* 32-bit residues (mod31): magic = floor(2^39 / m_i) + 1; c18 = 2^18 mod m_i, c36 = 2^36 mod m_i;
-     km = the least multiple of m_i that is at least 2^27 */
-  unsigned magic[kMaxMod], c18[kMaxMod], c36[kMaxMod], km[kMaxMod];
+     cneg = -2^54 mod m_i */
+  unsigned magic[kMaxMod], c18[kMaxMod], c36[kMaxMod], cneg[kMaxMod];
   double phi, plo; /* P as a double-double */
   int nmod, mb;
   /* w_i = y_i / m_i as a 128-bit binary fraction (floor(2^128 y_i / m_i)), least significant word
@@ -113,9 +113,10 @@ __device__ __forceinline__ unsigned mod31(unsigned x, unsigned m, unsigned magic
   return x - (__umulhi(x, magic) >> 7) * m;
 }
 
-/* 16 consecutive k of one row as signed integers: each u < 2^53 is held as 18-bit limbs
-   a0 + a1 2^18 + a2 2^36, so u = x (mod m) with x = a0 + a1 c18 + a2 c36 < 2^27 (c = 2^18, 2^36 mod m),
-   and -u = km - x (mod m) with km >= 2^27 a multiple of m: all 32-bit arithmetic. */
+/* 16 consecutive k of one row as signed integers (-1)^s u, u < 2^53. A negative value is held as
+   u' = 2^54 - u (so that -u = u' + e (mod m) with e = -2^54 mod m), and u' <= 2^54 as 18-bit limbs
+   a0 + a1 2^18 + a2 2^36: its residue is that of x = a0 + a1 c18 + a2 c36 + s e < 2^27
+   (c = 2^18, 2^36 mod m), all 32-bit arithmetic. */
 struct Limbs16 {
   unsigned a0[16], a1[16], a2[16], sg[16];
 };
@@ -123,7 +124,8 @@ struct Limbs16 {
 __device__ __forceinline__ void limbs16(const double (&v)[16], int erow, int mb, Limbs16& L) {
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    const unsigned long long u = aligned_int(v[j], erow, mb, L.sg[j]);
+    unsigned long long u = aligned_int(v[j], erow, mb, L.sg[j]);
+    if (L.sg[j]) u = (1ull << 54) - u;
     L.a0[j] = (unsigned)u & 0x3ffffu;
     L.a1[j] = (unsigned)(u >> 18) & 0x3ffffu;
     L.a2[j] = (unsigned)(u >> 36);
@@ -132,18 +134,14 @@ __device__ __forceinline__ void limbs16(const double (&v)[16], int erow, int mb,
 
 /* The 16 residues modulo m_i as bytes (k ascending). */
 __device__ __forceinline__ uint4 residue_bytes16(const Limbs16& L, const Oz2Consts& cs, int i) {
-  const unsigned m = cs.mod[i], mg = cs.magic[i], c1 = cs.c18[i], c2 = cs.c36[i], km = cs.km[i];
+  const unsigned m = cs.mod[i], mg = cs.magic[i], c1 = cs.c18[i], c2 = cs.c36[i], e = cs.cneg[i];
+  unsigned r[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) r[j] = mod31(L.a0[j] + L.a1[j] * c1 + L.a2[j] * c2 + L.sg[j] * e, m, mg);
   uint32_t w[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    uint32_t x = 0;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = q * 4 + b;
-      const unsigned t = L.a0[j] + L.a1[j] * c1 + L.a2[j] * c2;
-      x |= mod31(L.sg[j] ? km - t : t, m, mg) << (8 * b);
-    }
-    w[q] = x;
+    w[q] = __byte_perm(__byte_perm(r[4 * q], r[4 * q + 1], 0x0040u), __byte_perm(r[4 * q + 2], r[4 * q + 3], 0x0040u), 0x5410u);
   }
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
@@ -419,14 +417,19 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
   int ia[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) ia[v] = (i0 + v < M) ? ea[i0 + v] : 0;
-  for (int j = blockIdx.y; j < N; j += gridDim.y) {
+  /* V residues per word; the next column's loads are in flight while this column is computed */
+  unsigned res[kMaxMod], nxt[kMaxMod];
+  auto load = [&](unsigned (&dst)[kMaxMod], int j) {
     const size_t off = (size_t)j * M + i0;
-    unsigned res[kMaxMod]; /* V residues per word, every load in flight before the arithmetic starts */
 #pragma unroll
     for (int q = 0; q < kMaxMod; ++q) {
-      if (4 == V) res[q] = (q < cs.nmod) ? *reinterpret_cast<const unsigned*>(R + (size_t)q * plane + off) : 0u;
-      else res[q] = (q < cs.nmod) ? R[(size_t)q * plane + off] : 0u;
+      if (4 == V) dst[q] = (q < cs.nmod) ? *reinterpret_cast<const unsigned*>(R + (size_t)q * plane + off) : 0u;
+      else dst[q] = (q < cs.nmod) ? R[(size_t)q * plane + off] : 0u;
     }
+  };
+  if (blockIdx.y < N) load(res, blockIdx.y);
+  for (int j = blockIdx.y; j < N; j += gridDim.y) {
+    if (j + gridDim.y < N) load(nxt, j + gridDim.y);
     const int ib = eb[j];
     double* const cp = C + i0 + (long long)j * ldc;
 #pragma unroll
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
 #pragma unroll
       for (int q = 0; q < kMaxMod; ++q) {
         if (q < cs.nmod) {
-          const unsigned r = (res[q] >> (8 * v)) & 255u;
+          const unsigned r = __byte_perm(res[q], 0u, 0x4440u + v);
 #pragma unroll
           for (int w = 0; w < 4; ++w) acc[w] += (unsigned long long)r * cs.w[q][w];
         }
@@ -456,6 +459,8 @@ __global__ void __launch_bounds__(256) xs_oz2_reconstruct(const unsigned char* _
         cp[v] = (0.0 == beta) ? alpha * val : fma(alpha, val, beta * cp[v]);
       }
     }
+#pragma unroll
+    for (int q = 0; q < kMaxMod; ++q) res[q] = nxt[q];
   }
 }
 
@@ -552,7 +557,7 @@ int make_consts(int nmod, int K, Oz2Consts* cs) {
     cs->magic[i] = (unsigned)((1ull << 39) / m + 1ull);
     cs->c18[i] = (unsigned)((1ull << 18) % m);
     cs->c36[i] = (unsigned)((1ull << 36) % m);
-    cs->km[i] = (unsigned)(((1ull << 27) + m - 1) / m * m);
+    cs->cneg[i] = (unsigned)((m - (1ull << 54) % m) % m);
   }
   for (int i = 0; i < nmod; ++i) {
     const unsigned m = kModuli[i];
@@ -692,7 +697,9 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
   prof = xs_profile_begin(stream);
   const long long n = (long long)M * N;
   const int V = (0 == M % 4) ? 4 : 1;
-  const dim3 rgrid((unsigned)((M + 256 * V - 1) / (256 * V)), (unsigned)(N < 65535 ? N : 65535));
+  /* about four waves of resident blocks; each thread walks its columns */
+  const int rgx = (M + 256 * V - 1) / (256 * V), rgy = max(1, min(N, min(65535, 12 * xs_sm_count() / rgx)));
+  const dim3 rgrid((unsigned)rgx, (unsigned)rgy);
   if (4 == V) xs_oz2_reconstruct<4><<<rgrid, 256, 0, s>>>(rC, M, N, ea, eb, cs, alpha, beta, c, ldc);
   else xs_oz2_reconstruct<1><<<rgrid, 256, 0, s>>>(rC, M, N, ea, eb, cs, alpha, beta, c, ldc);
   r = (int)cudaGetLastError();
