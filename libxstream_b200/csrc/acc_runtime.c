@@ -20,8 +20,6 @@
 #include <stdio.h>
 #include <stdlib.h>
 
-#define XS_MAXDEV 64
-
 static pthread_mutex_t xs_lock = PTHREAD_MUTEX_INITIALIZER;
 static int xs_init_count = 0;
 static int xs_ndevices = -1;
@@ -107,6 +105,46 @@ int xs_ensure_device(void) {
 }
 
 int xs_active_device(void) { return xs_device; }
+
+int xs_device_slot(void) {
+  const int d = xs_device;
+  return (0 <= d && d < XS_MAXDEV) ? d : 0;
+}
+
+/* (device, kernel) -> dynamic shared memory limit already set */
+#define XS_FUNC_SLOTS 512
+static struct {
+  int dev, bytes;
+  const void* func;
+} xs_func_smem_set[XS_FUNC_SLOTS];
+static int xs_func_smem_n = 0;
+static pthread_mutex_t xs_func_lock = PTHREAD_MUTEX_INITIALIZER;
+
+int xs_func_smem(const void* func, size_t bytes) {
+  const int dev = xs_device_slot();
+  int i, r = 0, slot = -1;
+  if (bytes <= 48 * 1024) return 0; /* the default limit */
+  pthread_mutex_lock(&xs_func_lock);
+  for (i = 0; i < xs_func_smem_n; ++i) {
+    if (xs_func_smem_set[i].dev == dev && xs_func_smem_set[i].func == func) {
+      slot = i;
+      break;
+    }
+  }
+  if (0 > slot || xs_func_smem_set[slot].bytes < (int)bytes) {
+    r = (int)cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (cudaSuccess == r) {
+      if (0 > slot && xs_func_smem_n < XS_FUNC_SLOTS) slot = xs_func_smem_n++; /* a full table: set every time */
+      if (0 <= slot) {
+        xs_func_smem_set[slot].dev = dev;
+        xs_func_smem_set[slot].func = func;
+        xs_func_smem_set[slot].bytes = (int)bytes;
+      }
+    }
+  }
+  pthread_mutex_unlock(&xs_func_lock);
+  return r;
+}
 
 int xs_sm_count(void) {
   const int d = xs_device;

@@ -133,12 +133,8 @@ constexpr size_t smem_bytes() { return sizeof(double) * kStages * (kATile + kBTi
 template <int VEC>
 cudaError_t launch(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta, double* C,
   int ldc, cudaStream_t s) {
-  static int set = 0;
-  if (!set) {
-    const cudaError_t r = cudaFuncSetAttribute(xs_dgemm_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
-    if (cudaSuccess != r) return r;
-    set = 1;
-  }
+  const cudaError_t r = (cudaError_t)xs_func_smem((const void*)xs_dgemm_kernel<VEC>, smem_bytes());
+  if (cudaSuccess != r) return r;
   const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
   xs_dgemm_kernel<VEC><<<grid, kThreads, smem_bytes(), s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
   return cudaGetLastError();

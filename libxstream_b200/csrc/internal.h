@@ -18,6 +18,14 @@ extern "C" {
 int xs_ensure_device(void);
 /** Active device id (set by c_dbcsr_acc_set_active_device, default 0). */
 int xs_active_device(void);
+/** Device ids the runtime tracks per device (SM counts, pools, kernel set-up). */
+#define XS_MAXDEV 64
+/** The active device as an index of per-device caches, in [0, XS_MAXDEV). */
+int xs_device_slot(void);
+/** Make the dynamic shared memory limit of kernel `func` on the active device at least `bytes`
+    (function attributes are per device): set on first use per device and when a larger size is
+    asked for; returns a CUDA error code. */
+int xs_func_smem(const void* func, size_t bytes);
 /** Number of SMs of the active device (cached). */
 int xs_sm_count(void);
 /** Record a CUDA error code (nonzero) in the error slot; returns EXIT_FAILURE if code != 0. */

@@ -290,15 +290,9 @@ int grad_pass(Dev& d, int N, cudaStream_t s) {
 }
 
 int set_smem_attrs(void) {
-  static int done = 0;
-  if (!done) {
-    const int smem = (int)(sizeof(float) * NW);
-    int r = (int)cudaFuncSetAttribute(xs_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (0 == r) r = (int)cudaFuncSetAttribute(xs_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (0 != r) return r;
-    done = 1;
-  }
-  return 0;
+  const size_t smem = sizeof(float) * NW;
+  const int r = xs_func_smem((const void*)xs_mlp_fwd, smem);
+  return (0 != r) ? r : xs_func_smem((const void*)xs_mlp_bwd, smem);
 }
 
 /* ------------------------------------------------------------------ installed predictor table */

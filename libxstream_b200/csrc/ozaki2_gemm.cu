@@ -676,11 +676,7 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
   args.dev_err = xs_device_error_ptr();
   if (nullptr == args.dev_err) return (int)cudaErrorInvalidValue;
   const size_t smem = gemm_smem_bytes();
-  static int smem_set = 0;
-  if (!smem_set) {
-    if (0 != (r = (int)cudaFuncSetAttribute(xs_ozaki2_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return r;
-    smem_set = 1;
-  }
+  if (0 != (r = xs_func_smem((const void*)xs_ozaki2_gemm_kernel, smem))) return r;
   const int nkb = (K + kBK - 1) / kBK;
   const long long nunits = (long long)((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM) * nmod;
   const dim3 grid((unsigned)(nunits < xs_sm_count() ? nunits : xs_sm_count()));

@@ -456,11 +456,7 @@ int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, c
   }
   args.ngroups = ng;
   const size_t smem = gemm_smem_bytes();
-  static int smem_set = 0;
-  if (!smem_set) {
-    if (0 != (r = (int)cudaFuncSetAttribute(xs_ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return r;
-    smem_set = 1;
-  }
+  if (0 != (r = xs_func_smem((const void*)xs_ozaki_gemm_kernel, smem))) return r;
   const int nkb = (K + kBK - 1) / kBK;
   const dim3 grid(((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM));
   for (int kb0 = 0; kb0 < nkb; kb0 += kKChunkBlocks) {

@@ -532,11 +532,7 @@ int xs_launch_smm_ozaki(const int* dev_stack, int S, int m, int n, int k, const 
   xs_ozs_slice_pool<<<(nb + 1) / 2, 128, 0, s>>>(b, nb, (long long)k * n, 1, n, n, k, p.KP, p.rowsB, p.ns, dB, eB);
   if (0 != (r = (int)cudaGetLastError())) return r;
   xs_profile_end(prof, "ozaki_slice_pools", 0.0, 8.0 * ((double)na * m * k + (double)nb * k * n), stream);
-  static int smem_set = 0;
-  if (smem_set < (int)p.smem) {
-    if (0 != (r = (int)cudaFuncSetAttribute(xs_ozs_smm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem))) return r;
-    smem_set = (int)p.smem;
-  }
+  if (0 != (r = xs_func_smem((const void*)xs_ozs_smm_kernel, p.smem))) return r;
   const int part_max = xs_stack_group_max();
   for (int off = 0; off < S; off += part_max) {
     const int P = (S - off < part_max) ? S - off : part_max;

@@ -1101,13 +1101,11 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
 /* The combine kernel of one stack (CTA-crossing segments), MT x NT warp tiles. */
 template <int MT, int NT>
 cudaError_t launch_combine(const SmmPlan& pl, const StackTask& tk, const int* seglist, const unsigned* err, cudaStream_t s) {
-  static int csmem_set = 0;
   const int cgrid = max(1, min(pl.ngroups * pl.nsub, 2 * xs_sm_count()));
   const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (MT * NT * 2) * 32;
-  if (!csmem_set) {
-    const cudaError_t r = cudaFuncSetAttribute(xs_smm_combine_kernel<MT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+  {
+    const cudaError_t r = (cudaError_t)xs_func_smem((const void*)xs_smm_combine_kernel<MT, NT>, csmem);
     if (cudaSuccess != r) return r;
-    csmem_set = 1;
   }
   void* prof = xs_profile_begin(s);
   const cudaError_t r = pdl_launch(xs_smm_combine_kernel<MT, NT>, cgrid, 32 * kCombineWarps, csmem, s, tk, pl.W, seglist, err);
@@ -1119,14 +1117,9 @@ template <int M_, int N_, int K_, int MT, int NT, int KP>
 cudaError_t launch_dmma(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err, cudaStream_t s,
   int* occ) {
   cudaError_t r;
-  static int smem_set = 0; /* per template instance; setting it twice is harmless */
   const size_t smem = smm_smem_bytes<MT, NT>(pl.W);
-  if (smem > 48 * 1024 && smem_set < (int)smem) {
-    r = cudaFuncSetAttribute(xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      (int)smem);
-    if (cudaSuccess != r) return r;
-    smem_set = (int)smem;
-  }
+  r = (cudaError_t)xs_func_smem((const void*)xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, smem);
+  if (cudaSuccess != r) return r;
   if (nullptr != occ) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_dmma_kernel<M_, N_, K_, MT, NT, KP>, 32 * pl.W, smem);
   }
@@ -1144,13 +1137,9 @@ cudaError_t launch_staged(const SmmPlan& pl, const StackTask& tk, int* seglist, 
   int* occ) {
   using G = Staged<M_, N_, K_>;
   cudaError_t r;
-  static int smem_set = 0;
   const size_t smem = G::smem_bytes(pl.W, R);
-  if (smem > 48 * 1024 && smem_set < (int)smem) {
-    r = cudaFuncSetAttribute(xs_smm_staged_kernel<M_, N_, K_, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaSuccess != r) return r;
-    smem_set = (int)smem;
-  }
+  r = (cudaError_t)xs_func_smem((const void*)xs_smm_staged_kernel<M_, N_, K_, R>, smem);
+  if (cudaSuccess != r) return r;
   if (nullptr != occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_staged_kernel<M_, N_, K_, R>, 32 * pl.W, smem);
   if (1 != pl.nsub) return cudaErrorInvalidValue; /* one warp tile per C block */
   void* prof = xs_profile_begin(s);
@@ -1222,16 +1211,18 @@ size_t batch_smem_bytes(int grp) {
 
 template <int GRP>
 cudaError_t batch_prepare(int* occ) {
-  static int done = 0, occ_cached = 0;
+  static int occ_cached[XS_MAXDEV]; /* per device, 0 until set up */
+  const int dev = xs_device_slot();
   cudaError_t r = cudaSuccess;
-  if (!done) {
+  if (0 == occ_cached[dev]) {
     const size_t smem = batch_smem_bytes(GRP);
-    if (smem > 48 * 1024) r = cudaFuncSetAttribute(xs_smm_batch_kernel<GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaSuccess == r) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_cached, xs_smm_batch_kernel<GRP>, 32 * kBatchW, smem);
+    int o = 0;
+    r = (cudaError_t)xs_func_smem((const void*)xs_smm_batch_kernel<GRP>, smem);
+    if (cudaSuccess == r) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, xs_smm_batch_kernel<GRP>, 32 * kBatchW, smem);
     if (cudaSuccess != r) return r;
-    done = 1;
+    occ_cached[dev] = (o < 1) ? -1 : o;
   }
-  if (nullptr != occ) *occ = occ_cached;
+  if (nullptr != occ) *occ = (occ_cached[dev] < 0) ? 0 : occ_cached[dev];
   return r;
 }
 
@@ -1239,17 +1230,8 @@ cudaError_t batch_occupancy(int grp, int* occ) { return (0 == grp) ? batch_prepa
 
 template <int X>
 cudaError_t combine_prepare(void) {
-  static int done = 0;
-  if (!done) {
-    const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32;
-    if (csmem > 48 * 1024) {
-      const cudaError_t r = cudaFuncSetAttribute(xs_smm_combine_batch_kernel<X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int)csmem);
-      if (cudaSuccess != r) return r;
-    }
-    done = 1;
-  }
-  return cudaSuccess;
+  const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32;
+  return (cudaError_t)xs_func_smem((const void*)xs_smm_combine_batch_kernel<X>, csmem);
 }
 
 /* Persistent stack kernel of register group GRP over the tasks in bt (their own work queue). */
@@ -1784,17 +1766,11 @@ int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize
   cudaError_t r;
   void* const prof = xs_profile_begin(s);
   if (8 == esize) {
-    if (smem > 48 * 1024) {
-      r = cudaFuncSetAttribute(xs_transpose_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (cudaSuccess != r) return (int)r;
-    }
+    if (cudaSuccess != (r = (cudaError_t)xs_func_smem((const void*)xs_transpose_kernel<unsigned long long>, smem))) return (int)r;
     xs_transpose_kernel<unsigned long long><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned long long*)data, m, n, nb);
   }
   else if (4 == esize) {
-    if (smem > 48 * 1024) {
-      r = cudaFuncSetAttribute(xs_transpose_kernel<unsigned>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (cudaSuccess != r) return (int)r;
-    }
+    if (cudaSuccess != (r = (cudaError_t)xs_func_smem((const void*)xs_transpose_kernel<unsigned>, smem))) return (int)r;
     xs_transpose_kernel<unsigned><<<grid, threads, smem, s>>>(trs, offset, S, (unsigned*)data, m, n, nb);
   }
   else return (int)cudaErrorInvalidValue;

@@ -665,15 +665,16 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
 constexpr int kTileSmall = kSortThreads * 8, kTileLarge = kSortThreads * 16;
 
 int sort_grid_max(void) {
-  static int grid = 0;
-  if (0 == grid) {
+  static int grid[XS_MAXDEV]; /* per device, 0 until computed */
+  const int dev = xs_device_slot();
+  if (0 == grid[dev]) {
     int a = 0, b = 0;
     if (cudaSuccess != cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, xs_stack_group_kernel<8>, kSortThreads, 0)) a = 1;
     if (cudaSuccess != cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, xs_stack_group_kernel<16>, kSortThreads, 0)) b = 1;
     const int per_sm = a < b ? a : b;
-    grid = xs_sm_count() * (per_sm < 1 ? 1 : per_sm);
+    grid[dev] = xs_sm_count() * (per_sm < 1 ? 1 : per_sm);
   }
-  return grid;
+  return grid[dev];
 }
 
 /* Tiles of a batch: kTileSmall entries each, or kTileLarge when the small tiles do not fit on the
@@ -725,9 +726,9 @@ int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long*
 int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, SortCtl* ctl, int ncta,
   cudaStream_t s) {
-  static int ok[kClusterMax + 1]; /* per cluster size: 0 unknown, 1 supported, -1 not */
+  static int ok[XS_MAXDEV][kClusterMax + 1]; /* per device and cluster size: 0 unknown, 1 supported, -1 not */
   auto kernel = xs_stack_group_cluster_kernel<kClE>;
-  int* const okp = &ok[ncta];
+  int* const okp = &ok[xs_device_slot()][ncta];
   const size_t smem = kClSmem;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)ncta);
