@@ -1,8 +1,8 @@
 """GPU tests of the Ozaki scheme-2 (Chinese remainder) FP64 GEMM on the int8 tensor cores
 (libxstream_b200_ozaki2_gemm): the device result against the CPU restatement of the same scheme
-(same integers, same moduli, exact CRT in Python integers; only the device's double-double
-reconstruction rounds), and the error of the scheme against a plain FP64 GEMM (numpy/BLAS) per
-modulus count."""
+(same integers, same moduli, exact CRT in Python integers; only the device's reconstruction, a
+128-bit binary fraction times P, rounds), and the error of the scheme against a plain FP64 GEMM
+(numpy/BLAS) per modulus count."""
 from __future__ import annotations
 
 import numpy as np
@@ -13,7 +13,7 @@ from oracle import ozaki2 as O
 
 pytestmark = pytest.mark.gpu
 
-RECON_TOL = 4e-16  # device vs exact scheme, relative to the largest |C|: double-double CRT rounding
+RECON_TOL = 4e-16  # device vs exact scheme, relative to the largest |C|: reconstruction rounding
 FP64_TOL = 1e-14   # scheme with all 53 bits vs FP64 GEMM (numpy), relative max-norm
 
 
@@ -90,6 +90,21 @@ def test_long_k_runs_in_chunks(acc):
     b = g.uniform(-1, 1, size=(K, N))
     got = run(A, stream, "N", "N", M, N, K, a, b, np.zeros((M, N)))
     assert relerr(got, a @ b) <= FP64_TOL
+
+
+def test_long_k_ragged_rows_match_row_subset(acc):
+    """K = 40000 (two launches accumulating residues) over three row tiles, the last one ragged:
+    the first 128 rows of the 300-row product equal the 128-row product of the same rows bit for
+    bit (each row keeps its own scaling, tiles do not interact)."""
+    A, stream = acc
+    M, N, K = 300, 100, 40000
+    g = W.rng(14)
+    a = g.uniform(-1, 1, size=(M, K))
+    b = g.uniform(-1, 1, size=(K, N))
+    tall = run(A, stream, "N", "N", M, N, K, a, b, np.zeros((M, N)))
+    short = run(A, stream, "N", "N", 128, N, K, np.ascontiguousarray(a[:128]), b, np.zeros((128, N)))
+    assert relerr(tall, a @ b) <= FP64_TOL
+    assert np.array_equal(tall[:128], short)
 
 
 def test_zero_rows_and_special_sizes(acc):
