@@ -27,8 +27,8 @@
  * units (modulus, 128 x 256 tile of C) taken modulus-major and strided by the grid: warp 0 streams
  * the k-blocks of both operands' residue planes into a 4-stage shared-memory ring with TMA (128-byte
  * swizzle); warp 1 owns two 128 x 256 int32 accumulators in tensor memory and one lane issues the
- * MMAs; warps 2-5 reduce a finished accumulator modulo m_i and store the bytes while the tensor cores
- * work on the next unit. Every mbarrier wait is bounded (per-call abort word, library device error
+ * MMAs; warps 2-9 (two per tensor-memory lane quarter, one column half each) reduce a finished
+ * accumulator modulo m_i and store the bytes while the tensor cores work on the next unit. Every mbarrier wait is bounded (per-call abort word, library device error
  * word).
  */
 #include "internal.h"
@@ -48,7 +48,7 @@ using namespace xs_oz;
 
 constexpr int kMaxMod = 20;
 constexpr int kBM = 128, kBN = 256, kBK = 128, kStages = 4;
-constexpr int kThreads = 192;
+constexpr int kThreads = 320; /* producer, MMA issuer, 8 epilogue warps */
 constexpr int kGroupM = 8;
 /* k-blocks per launch: 32768 * 255^2 < 2^31 keeps every int32 sum exact */
 constexpr int kKChunkBlocks = 32768 / kBK;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&accf[i], 1);
-      mbar_init(&acce[i], 128);
+      mbar_init(&acce[i], kThreads - 64);
     }
     fence_barrier_init();
     prefetch_tensormap(&mapA);
@@ -340,8 +340,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   }
-  else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; thread = one row of the tile */
-    const int qd = warp & 3;
+  else { /* epilogue: warps 2..9, tensor-memory lane quarter warp % 4 and column half (warp - 2) / 4;
+            thread = one row of the tile, 128 columns */
+    const int qd = warp & 3, cb = ((warp - 2) >> 2) * (kBN / 2);
     for (int u = blockIdx.x, i = 0; u < nunits; u += gridDim.x, ++i) {
       const int buf = i & 1, use = i >> 1;
       int q, m0, n0;
@@ -353,19 +354,26 @@ __global__ void __launch_bounds__(kThreads, 1)
       const unsigned m = args.mod[q];
       const unsigned mg = args.magic[q];
       unsigned char* const plane = args.R + (size_t)q * args.M * args.N;
-      for (int c0 = 0; c0 < kBN; c0 += 32) {
+      for (int c0 = cb; c0 < cb + kBN / 2; c0 += 32) {
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(buf * kBN + c0), v);
         tmem_ld_wait();
         if (rok) {
           const int ncol = min(32, args.N - (n0 + c0));
           unsigned char* const dst = plane + row + (size_t)(n0 + c0) * args.M;
-          unsigned prev[32];
+          if (!args.first) { /* a later k-chunk: add the residues so far */
 #pragma unroll
-          for (int j = 0; j < 32; ++j) prev[j] = (j < ncol && !args.first) ? dst[(size_t)j * args.M] : 0u;
+            for (int j = 0; j < 32; ++j) v[j] += (j < ncol) ? dst[(size_t)j * args.M] : 0u;
+          }
+          if (32 == ncol) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            if (j < ncol) dst[(size_t)j * args.M] = (unsigned char)mod31(v[j] + prev[j], m, mg); /* < 2^31 */
+            for (int j = 0; j < 32; ++j) dst[(size_t)j * args.M] = (unsigned char)mod31(v[j], m, mg); /* < 2^31 */
+          }
+          else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              if (j < ncol) dst[(size_t)j * args.M] = (unsigned char)mod31(v[j], m, mg);
+            }
           }
         }
       }
