@@ -3,7 +3,7 @@
  *
  * C = alpha * op(A) * op(B) + beta * C, FP64, column-major (BLAS conventions), the second scheme of
  * the reference's Ozaki sample (samples/ozaki/kernels/ozaki2_int8.cl:13-45, host set-up
- * samples/ozaki/ozaki_opencl.c:415-460). Each row of op(A) and each column of op(B) is scaled by its
+ * samples/ozaki/ozaki_opencl.c:406-426). Each row of op(A) and each column of op(B) is scaled by its
  * largest power of two and turned into integers of MB bits (the aligned significands of
  * xs_oz::ieee_split, truncated to MB bits; MB = 53 keeps every bit of the largest entry). The exact
  * integer product A_int * B_int is then computed modulo q moduli m_1..m_q (pairwise coprime, at most

@@ -1,13 +1,13 @@
 """CPU restatement of the Ozaki scheme-2 (Chinese remainder) FP64 GEMM (test infrastructure only).
 
 The reference's scheme 2 (samples/ozaki/kernels/ozaki2_int8.cl:13-45; moduli count and input
-mantissa bits, samples/ozaki/ozaki_opencl.c:415-460): each row of A and each column of B is scaled
+mantissa bits, samples/ozaki/ozaki_opencl.c:406-426): each row of A and each column of B is scaled
 by its largest power of two and truncated to a signed integer of `mb` bits (the aligned significand
 of samples/ozaki/kernels/ozaki_common.cl:789-806, cut to mb bits); the integer product is taken
 modulo every modulus (one 8-bit GEMM each on the device), reconstructed exactly by the CRT, centred
 to [-P/2, P/2) and scaled back. This restatement computes the residue products with numpy int64
 and the reconstruction with Python integers, so it is the scheme's exact result (the device's
-double-double reconstruction differs from it by rounding only). The moduli are this build's own
+reconstruction, a 128-bit binary fraction of x / P times P, differs from it by rounding only). The moduli are this build's own
 set (pairwise coprime, <= 256); the reference picks its own.
 """
 from __future__ import annotations
