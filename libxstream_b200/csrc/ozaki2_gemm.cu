@@ -23,13 +23,13 @@
  * Device layout: residue planes rA[q][M][Kp] and rB[q][N][Kp] (u8, K contiguous, zero padded),
  * exponents ea[M], eb[N], residues of C R[q][N][M] (u8, column-major per modulus).
  *
- * GEMM kernel: persistent, one CTA per SM, 6 warps, the pipeline of the scheme-1 kernel over work
+ * GEMM kernel: persistent, one CTA per SM, 10 warps, the pipeline of the scheme-1 kernel over work
  * units (modulus, 128 x 256 tile of C) taken modulus-major and strided by the grid: warp 0 streams
  * the k-blocks of both operands' residue planes into a 4-stage shared-memory ring with TMA (128-byte
  * swizzle); warp 1 owns two 128 x 256 int32 accumulators in tensor memory and one lane issues the
  * MMAs; warps 2-9 (two per tensor-memory lane quarter, one column half each) reduce a finished
- * accumulator modulo m_i and store the bytes while the tensor cores work on the next unit. Every mbarrier wait is bounded (per-call abort word, library device error
- * word).
+ * accumulator modulo m_i and store the bytes while the tensor cores work on the next unit. Every
+ * mbarrier wait is bounded (per-call abort word, library device error word).
  */
 #include "internal.h"
 #include "tc_ptx.cuh"
