@@ -168,9 +168,13 @@ def cpu_baseline(case, seconds: float) -> dict:
         el = time.perf_counter() - t0
         if el >= seconds:
             break
-    return {"value": case.flops * reps / el * 1e-9, "unit": UNIT, "cores": threads, "kind": "port",
+    value = case.flops * reps / el * 1e-9
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "per_core": value / threads,
+            "busiest_thread_load": oracle.fast_balance(case.S, threads),
             "sample": f"{reps} repetitions of the full {case.m}x{case.n}x{case.k} stack ({case.S} triples), "
-                      f"{el:.1f} s, OpenMP register-tiled restatement (oracle/smm_oracle.c: oracle_smm_f64_fast)"}
+                      f"{el:.1f} s, OpenMP register-tiled restatement (oracle/smm_oracle.c: oracle_smm_f64_fast): "
+                      "stack grouped by C, equal contiguous ranges per thread, boundary segments in private "
+                      "partial tiles"}
 
 
 def workload_config(case) -> dict:
@@ -202,9 +206,11 @@ def run_reference(args, d: Dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(case),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "per_core": value / threads,
+                             "busiest_thread_load": oracle.fast_balance(case.S, threads),
                              "sample": f"the full stack per step, {args.steps} steps; the reference's CPU path "
-                                       "(LIBXS, OpenCL) cannot be built here, so its oracle restatement runs"},
+                                       "(LIBXS, OpenCL) cannot be built here, so its oracle restatement runs "
+                                       "(grouped by C, equal contiguous ranges per thread)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -363,6 +369,8 @@ def run_b200(args, d: Dist):
     contract_tf = min(peak or float("inf"), hbm_gbs * ai * 1e-3)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved and peak and peak > 0 else None, "traffic": traffic,
+                "traffic_source": "not measured in this run: dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "stack-kernel launch from a committed ncu capture (profiles/traffic.json)",
                 "kernel": "xs_smm_staged_kernel<23,23,23,2> (stack kernel of this shape)",
                 "launches_timed": smm.get("launches"), "peak_source": "FP64 DMMA peak measured live on this GPU "
                 "(libxstream_b200_fp64_peak: mma.sync m8n8k4 f64 loop)",

@@ -39,10 +39,27 @@ int libxstream_b200_process_batch(const libxstream_b200_stack_t* stacks, int nst
 int libxstream_b200_process_suitable(
   c_dbcsr_acc_bool_t def_mnk, libsmm_acc_data_t datatype, int stack_size, int m, int n, int k, int max_kernel_dim);
 
-/** Device-side error word of the library (bit 0: a grid barrier of the grouping sort timed out, the
-    affected call then wrote nothing); reset != 0 clears it. Synchronises the device. No counterpart
-    in the reference. */
+/** Device-side error word of the library: bit 0 = a grid barrier of the grouping sort timed out (the
+    affected call then wrote nothing), bit 2 = a pipeline wait of an Ozaki kernel timed out, bit 3 = an
+    Ozaki stack entry with an offset that is not a multiple of the block size, bit 4 = a wait of the
+    staged stack kernel for its block copies timed out. reset != 0 clears it. Synchronises the device.
+    The ACC calls report the same word: c_dbcsr_acc_stream_sync and c_dbcsr_acc_device_synchronize
+    read it after the synchronisation and return nonzero (error slot: cudaErrorTimeout) when it is
+    set; from then on libsmm_acc_process, libsmm_acc_transpose and the batch, DBM and allocation-free
+    stack calls return nonzero without doing work, until c_dbcsr_acc_clear_errors consumes the word
+    (as the reference's error slot is consumed, src/libxstream_dbcsr.c:57-62). No counterpart in the
+    reference for the word itself. */
 int libxstream_b200_device_error(int reset);
+
+/** Bound, in GPU clock cycles, of every pipeline wait of the kernels launched after this call (the
+    staged stack kernel's waits for its block copies and the Ozaki kernels' mbarrier waits); cycles
+    <= 0 restores the default of 4e9 cycles (about two seconds). A wait that runs out sets its bit
+    in the device error word and the kernel stops early (the C blocks of that call are then
+    incomplete; nothing faults or hangs). A launch
+    captured into a CUDA graph keeps the bound that was set when it was captured. Meant for tests of
+    the error path and for callers that want a shorter bound. No counterpart in the reference. */
+void libxstream_b200_set_wait_limit(long long cycles);
+long long libxstream_b200_get_wait_limit(void);
 
 /** Last CUDA error code recorded by the library (0 if none); cleared by c_dbcsr_acc_clear_errors.
     Corresponds to the reference's error slot (libxstream/libxstream_opencl.h:156-194). */
@@ -103,7 +120,10 @@ int libxstream_b200_graph_destroy(void* graph_exec);
     per call: applications that reserve nearly all device memory for their own allocator at
     start-up, or code that must not take the driver's allocation locks or risk the device
     synchronisation a growing memory pool or cudaFree can cause. Same arguments, results and
-    return codes as libsmm_acc_process; its scratch is a fixed 8 MiB device array inside the
+    return codes as libsmm_acc_process, with two differences: it never hands the stack to a DBM
+    launch hook (libxstream_b200_set_dbm_launch_fn), and it never runs the exhaustive autotuner
+    (tuning allocates), so with LIBXSTREAM_B200_AUTOTUNE=1 a shape not yet tuned runs with the
+    predicted or default parameters. Its scratch is a fixed 8 MiB device array inside the
     library (held by every GPU that uses the library until the process exits), so a stack that
     needs more (libxstream_b200_process_scratch_bytes) is rejected with a nonzero return and a
     message. The first call on a device looks up the array's device address: make it before any

@@ -147,6 +147,8 @@ SIGNATURES = {
     "libxstream_b200_noalloc_scratch_bytes": (ctypes.c_size_t, []),
     "libxstream_b200_process_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "libxstream_b200_device_error": (ctypes.c_int, [ctypes.c_int]),
+    "libxstream_b200_set_wait_limit": (None, [ctypes.c_longlong]),
+    "libxstream_b200_get_wait_limit": (ctypes.c_longlong, []),
     "libxstream_b200_process_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
 }
 

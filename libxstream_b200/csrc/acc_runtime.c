@@ -30,6 +30,13 @@ static int xs_smcount[XS_MAXDEV];
 static int xs_pool_ready[XS_MAXDEV];
 static int xs_alloc_fail_countdown = 0;
 static __thread int xs_thread_device = -1;
+/* Bound of the kernels' pipeline waits in clock cycles (0: XS_DEFAULT_WAIT_LIMIT). */
+static long long xs_wait_cycles = 0;
+/* Set once a synchronisation found the device error word non-zero; cleared by
+   c_dbcsr_acc_clear_errors. While it is set, the stack calls refuse work. */
+static int xs_device_fault = 0;
+/* Pinned host words that receive copies of each device's error word at stream synchronisation. */
+static unsigned* xs_err_mirror[XS_MAXDEV];
 
 int xs_verbosity(void) {
   if (0 > xs_verbose) {
@@ -60,6 +67,49 @@ int xs_consume_error(void) {
 }
 
 void xs_inject_alloc_failure(int nth) { xs_alloc_fail_countdown = nth; }
+
+long long xs_wait_limit(void) {
+  const long long w = __atomic_load_n(&xs_wait_cycles, __ATOMIC_RELAXED);
+  return (0 < w) ? w : XS_DEFAULT_WAIT_LIMIT;
+}
+
+void libxstream_b200_set_wait_limit(long long cycles) { __atomic_store_n(&xs_wait_cycles, 0 < cycles ? cycles : 0, __ATOMIC_RELAXED); }
+
+long long libxstream_b200_get_wait_limit(void) { return xs_wait_limit(); }
+
+int xs_device_fault_pending(void) { return __atomic_load_n(&xs_device_fault, __ATOMIC_RELAXED); }
+
+/* A device error word read back from the GPU: non-zero means a kernel's bounded wait gave up (or a
+   kernel found an input it could not use) and its results are incomplete. That becomes the error
+   slot's code (cudaErrorTimeout), a nonzero return, and the sticky flag the stack calls check. */
+static int xs_device_status(unsigned word) {
+  if (0 == word) return EXIT_SUCCESS;
+  __atomic_store_n(&xs_device_fault, 1, __ATOMIC_RELAXED);
+  xs_error = (int)cudaErrorTimeout;
+  if (0 != xs_verbosity()) {
+    fprintf(stderr, "ERROR ACC/B200: a kernel reported a device-side error (error word 0x%x): results are incomplete\n", word);
+  }
+  return EXIT_FAILURE;
+}
+
+/* Pinned host word of the active device for copies of its error word (allocated on first use). */
+static unsigned* xs_error_mirror(void) {
+  const int d = xs_device_slot();
+  unsigned* m = __atomic_load_n(&xs_err_mirror[d], __ATOMIC_ACQUIRE);
+  if (NULL == m) {
+    void* p = NULL;
+    pthread_mutex_lock(&xs_lock);
+    m = xs_err_mirror[d];
+    if (NULL == m && cudaSuccess == cudaHostAlloc(&p, 64, cudaHostAllocPortable)) {
+      *(volatile unsigned*)p = 0;
+      m = (unsigned*)p;
+      __atomic_store_n(&xs_err_mirror[d], m, __ATOMIC_RELEASE);
+    }
+    pthread_mutex_unlock(&xs_lock);
+    if (NULL == m) (void)cudaGetLastError();
+  }
+  return m;
+}
 
 static int xs_count_devices(void) {
   if (0 > xs_ndevices) {
@@ -200,6 +250,12 @@ int c_dbcsr_acc_finalize(void) {
 void c_dbcsr_acc_clear_errors(void) {
   xs_error = 0;
   (void)cudaGetLastError();
+  if (0 < xs_init_count && EXIT_SUCCESS == xs_ensure_device()) { /* consume the device error word */
+    unsigned w = 0;
+    if (cudaSuccess != xs_device_error_read(&w) || 0 != w) (void)xs_device_error_clear();
+    (void)cudaGetLastError();
+  }
+  __atomic_store_n(&xs_device_fault, 0, __ATOMIC_RELAXED);
 }
 
 /* ---------------------------------------------------------------------------------- devices */
@@ -218,8 +274,12 @@ int c_dbcsr_acc_set_active_device(int device_id) {
 }
 
 int c_dbcsr_acc_device_synchronize(void) {
+  unsigned w = 0;
+  int r;
   if (EXIT_SUCCESS != xs_ensure_device()) return EXIT_FAILURE;
-  return xs_record_error((int)cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  r = xs_record_error((int)cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  if (EXIT_SUCCESS == r) r = xs_record_error(xs_device_error_read(&w), "device error word");
+  return (EXIT_SUCCESS == r) ? xs_device_status(w) : r;
 }
 
 /* ---------------------------------------------------------------------------------- streams */
@@ -255,10 +315,19 @@ int c_dbcsr_acc_stream_destroy(void* stream) {
   return xs_record_error((int)cudaStreamDestroy((cudaStream_t)stream), "cudaStreamDestroy");
 }
 
+/* The device error word is copied into a pinned host word on the same stream just before the
+   synchronisation, so reading it costs no extra round trip. */
 int c_dbcsr_acc_stream_sync(void* stream) {
+  const cudaStream_t s = NULL != stream ? (cudaStream_t)stream : cudaStreamPerThread;
+  unsigned* mirror;
+  int r;
   if (EXIT_SUCCESS != xs_ensure_device()) return EXIT_FAILURE;
-  return xs_record_error(
-    (int)cudaStreamSynchronize(NULL != stream ? (cudaStream_t)stream : cudaStreamPerThread), "cudaStreamSynchronize");
+  mirror = xs_error_mirror();
+  if (NULL != mirror && EXIT_SUCCESS != xs_record_error(xs_device_error_fetch(mirror, s), "device error word")) {
+    return EXIT_FAILURE;
+  }
+  r = xs_record_error((int)cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return (EXIT_SUCCESS == r && NULL != mirror) ? xs_device_status(*(volatile unsigned*)mirror) : r;
 }
 
 int c_dbcsr_acc_stream_wait_event(void* stream, void* event) {

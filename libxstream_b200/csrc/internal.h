@@ -45,6 +45,13 @@ int xs_scratch_alloc(void** ptr, size_t nbytes, void* stream);
 int xs_scratch_free(void* ptr, void* stream);
 /** Test hook: make the n-th following scratch allocation fail (0 disables). */
 void xs_inject_alloc_failure(int nth);
+/** Default bound of a kernel's pipeline wait, in clock cycles (about two seconds at 1.965 GHz). */
+#define XS_DEFAULT_WAIT_LIMIT 4000000000LL
+/** Bound of the kernels' pipeline waits in clock cycles, passed to every launch that has such waits
+    (libxstream_b200_set_wait_limit; XS_DEFAULT_WAIT_LIMIT unless set). */
+long long xs_wait_limit(void);
+/** 1 once a synchronisation found the device error word set, until c_dbcsr_acc_clear_errors. */
+int xs_device_fault_pending(void);
 
 /* ------------------------------------------------------------------ launch profile (profile.c) */
 
@@ -100,6 +107,11 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int stack_size, int format, doubl
 
 /** Device address of the library's device error word (current device). */
 unsigned* xs_device_error_ptr(void);
+/** Enqueue a copy of the current device's error word into host memory (pinned) on the stream. */
+int xs_device_error_fetch(unsigned* host_dst, void* stream);
+/** Read (synchronously) / reset the current device's error word; return a cudaError_t value. */
+int xs_device_error_read(unsigned* value);
+int xs_device_error_clear(void);
 
 /** Ozaki scheme-1 FP64 GEMM on the int8 tensor cores (ozaki_gemm.cu): C = alpha*op(A)*op(B) + beta*C,
     column-major, nslices in 1..8, slice pairs with sa + sb <= cutoff (cutoff < 0: all pairs).

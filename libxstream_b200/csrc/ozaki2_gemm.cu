@@ -232,6 +232,7 @@ struct Oz2GemmArgs {
   unsigned char* R; /* [nmod][N][M] */
   unsigned* abort;
   unsigned* dev_err;
+  long long wait_limit; /* bound of every pipeline wait, clock cycles */
 };
 
 constexpr size_t gemm_smem_bytes() {
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
           const int stage = it % kStages;
           const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-          if (!(ok = mbar_wait(&empty[stage], ph ^ 1u, abort, 1u))) break;
+          if (!(ok = mbar_wait(&empty[stage], ph ^ 1u, abort, 1u, args.wait_limit))) break;
           mbar_arrive_expect_tx(&full[stage], kATileBytes + kBTileBytes);
           tma_load_3d(sA + stage * kATileBytes, &mapA, kb * kBK, m0, q, &full[stage]);
           tma_load_3d(sB + stage * kBTileBytes, &mapB, kb * kBK, n0, q, &full[stage]);
@@ -319,14 +320,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int u = blockIdx.x, i = 0; u < nunits && ok; u += gridDim.x, ++i) {
         const int buf = i & 1, use = i >> 1;
-        if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u))) break;
+        if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u, args.wait_limit))) break;
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(buf * kBN);
         uint32_t acc = 0;
         for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
           const int stage = it % kStages;
           const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-          if (!(ok = mbar_wait(&full[stage], ph, abort, 2u))) break;
+          if (!(ok = mbar_wait(&full[stage], ph, abort, 2u, args.wait_limit))) break;
           tc_fence_after();
           const uint32_t a0 = smem_u32(sA + stage * kATileBytes), b0 = smem_u32(sB + stage * kBTileBytes);
 #pragma unroll
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       unit_coords(u, ntiles, ntm, ntn, q, m0, n0);
       const int row = m0 + qd * 32 + lane;
       const bool rok = row < args.M;
-      if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u)) break;
+      if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u, args.wait_limit)) break;
       tc_fence_after();
       const unsigned m = args.mod[q];
       const unsigned mg = args.magic[q];
@@ -682,6 +683,7 @@ int xs_ozaki2_gemm(char transa, char transb, int M, int N, int K, double alpha, 
   args.R = rC;
   args.abort = abort;
   args.dev_err = xs_device_error_ptr();
+  args.wait_limit = xs_wait_limit();
   if (nullptr == args.dev_err) return (int)cudaErrorInvalidValue;
   const size_t smem = gemm_smem_bytes();
   if (0 != (r = xs_func_smem((const void*)xs_ozaki2_gemm_kernel, smem))) return r;

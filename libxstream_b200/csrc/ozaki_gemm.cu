@@ -159,6 +159,7 @@ struct OzGemmArgs {
   long long ldc;
   unsigned* abort; /* per-call abort word (zeroed by the host before the first launch) */
   unsigned* dev_err;
+  long long wait_limit; /* bound of every pipeline wait, clock cycles */
   unsigned char sa[kMaxPairs], sb[kMaxPairs];
   OzGroup g[kMaxGroups];
 };
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
             const int stage = it % kStages;
             const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-            if (!(ok = mbar_wait(&empty[stage], ph ^ 1u, abort, 1u))) break;
+            if (!(ok = mbar_wait(&empty[stage], ph ^ 1u, abort, 1u, args.wait_limit))) break;
             mbar_arrive_expect_tx(&full[stage], kATileBytes + kBTileBytes);
             tma_load_3d(sA + stage * kATileBytes, &mapA, kb * kBK, m0, za, &full[stage]);
             tma_load_3d(sB + stage * kBTileBytes, &mapB, kb * kBK, n0, zb, &full[stage]);
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       bool ok = true;
       for (int g = 0; g < args.ngroups && ok; ++g) {
         const int buf = g & 1, use = g >> 1;
-        if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u))) break;
+        if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u, args.wait_limit))) break;
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(buf * kBN);
         uint32_t acc = 0;
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           for (int kb = args.kb0; kb < args.kb1; ++kb, ++it) {
             const int stage = it % kStages;
             const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-            if (!(ok = mbar_wait(&full[stage], ph, abort, 2u))) break;
+            if (!(ok = mbar_wait(&full[stage], ph, abort, 2u, args.wait_limit))) break;
             tc_fence_after();
             const uint32_t a0 = smem_u32(sA + stage * kATileBytes), b0 = smem_u32(sB + stage * kBTileBytes);
 #pragma unroll
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const int ear = rok ? args.ea[row] : 0;
     for (int g = 0; g < args.ngroups; ++g) {
       const int buf = g & 1, use = g >> 1;
-      if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u)) break;
+      if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u, args.wait_limit)) break;
       tc_fence_after();
       const int eshift = args.g[g].eshift;
       const bool beta_now = (0 != args.first) && (0 == g);
@@ -436,6 +437,7 @@ int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, c
   args.ldc = ldc;
   args.abort = abort;
   args.dev_err = xs_device_error_ptr();
+  args.wait_limit = xs_wait_limit();
   if (nullptr == args.dev_err) return (int)cudaErrorInvalidValue;
   int np = 0, ng = 0;
   for (int d = 0; d <= cutoff; ++d) { /* pairs ordered by anti-diagonal, one accumulation group each */

@@ -120,6 +120,7 @@ struct OzSmmArgs {
   double* pieces; /* [chunk][2][m*n] */
   unsigned* abort;
   unsigned* dev_err;
+  long long wait_limit; /* bound of every pipeline wait, clock cycles */
 };
 
 __device__ __forceinline__ double pow2_or_zero(int e) { /* 2^(e - 1029) for a biased exponent e, 0 for e < 7 */
@@ -205,12 +206,12 @@ __global__ void __launch_bounds__(kThreads, 1) xs_ozs_smm_kernel(const __grid_co
         const int ab = s_blk[e].x, bb = s_blk[e].y;
         { /* exponents of the entry's A rows and B columns into the exponent ring */
           const int xs = e % kXSlots;
-          if (!mbar_wait(&xempty[xs], ((uint32_t)(e / kXSlots) & 1u) ^ 1u, abort, 1u)) break;
+          if (!mbar_wait(&xempty[xs], ((uint32_t)(e / kXSlots) & 1u) ^ 1u, abort, 1u, g.wait_limit)) break;
           mbar_arrive_expect_tx(&xfull[xs], 512);
           bulk_load(xring + xs * 128, g.eA + (size_t)ab * 64, 256, &xfull[xs]);
           bulk_load(xring + xs * 128 + 64, g.eB + (size_t)bb * 64, 256, &xfull[xs]);
         }
-        if (!mbar_wait(&empty[stage], ph ^ 1u, abort, 1u)) break;
+        if (!mbar_wait(&empty[stage], ph ^ 1u, abort, 1u, g.wait_limit)) break;
         unsigned char* const st = smem + (size_t)stage * g.stage_bytes;
         const unsigned bytesA = (unsigned)g.ns * g.sliceA, bytesB = (unsigned)g.ns * g.sliceB;
         mbar_arrive_expect_tx(&full[stage], bytesA + bytesB);
@@ -227,13 +228,13 @@ __global__ void __launch_bounds__(kThreads, 1) xs_ozs_smm_kernel(const __grid_co
       for (int e = 0; e < nent && ok; ++e) {
         const int stage = e % g.nstages;
         const uint32_t ph = (uint32_t)(e / g.nstages) & 1u;
-        if (!(ok = mbar_wait(&full[stage], ph, abort, 2u))) break;
+        if (!(ok = mbar_wait(&full[stage], ph, abort, 2u, g.wait_limit))) break;
         tc_fence_after();
         const uint32_t sA = smem_u32(smem + (size_t)stage * g.stage_bytes);
         const uint32_t sB = sA + g.offB;
         for (int w = 0; w < g.nwin && ok; ++w, ++grp) {
           const int buf = grp % g.nbuf, use = grp / g.nbuf;
-          if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u))) break;
+          if (!(ok = mbar_wait(&acce[buf], ((uint32_t)use & 1u) ^ 1u, abort, 2u, g.wait_limit))) break;
           tc_fence_after();
           const OzWin& wn = g.win[w];
           const uint32_t idesc = idesc_i8(64, wn.W * g.rowsB);
@@ -310,12 +311,12 @@ __global__ void __launch_bounds__(kThreads, 1) xs_ozs_smm_kernel(const __grid_co
         seg_key = key;
       }
       const int xs = e % kXSlots;
-      if (!(ok = mbar_wait(&xfull[xs], (uint32_t)(e / kXSlots) & 1u, abort, 8u))) break;
+      if (!(ok = mbar_wait(&xfull[xs], (uint32_t)(e / kXSlots) & 1u, abort, 8u, g.wait_limit))) break;
       const int* const xe = xring + xs * 128;
       const double rs = rok ? pow2_or_zero(xe[row]) : 0.0;
       for (int w = 0; w < g.nwin; ++w, ++grp) {
         const int buf = grp % g.nbuf, use = grp / g.nbuf;
-        if (!(ok = mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u))) break;
+        if (!(ok = mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u, g.wait_limit))) break;
         tc_fence_after();
         const OzWin& wn = g.win[w];
         const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * g.bufcols);
@@ -581,6 +582,7 @@ int xs_launch_smm_ozaki(const int* dev_stack, int S, int m, int n, int k, const 
     g.pieces = (double*)(base + l.pieces);
     g.abort = abort;
     g.dev_err = xs_device_error_ptr();
+    g.wait_limit = xs_wait_limit();
     if (nullptr == g.dev_err) return (int)cudaErrorInvalidValue;
     prof = xs_profile_begin(stream);
     xs_ozs_smm_kernel<<<g.nchunks, kThreads, p.smem, s>>>(g);

@@ -17,6 +17,9 @@
  * takes its host path, which the reference also does when built without OPENCL_LIBSMM_F32.
  * Parameters come from the table (B200SMM_PARAMS=<csv> loads one, =0 disables it) or from the
  * default heuristic; LIBXSTREAM_B200_VERBOSE=2 prints the choice per shape, 3 prints every launch.
+ * Device-side errors (a bounded wait that gave up) are read at the synchronisation points
+ * (c_dbcsr_acc_stream_sync, c_dbcsr_acc_device_synchronize); once one was seen, the stack calls
+ * here return EXIT_FAILURE without work until c_dbcsr_acc_clear_errors.
  */
 #include "internal.h"
 #include "../../include/libsmm_acc.h"
@@ -153,6 +156,7 @@ static int xs_process_format(const int* dev_param_stack, int stack_size, int for
     return (0 < stack_size) ? -1 : EXIT_SUCCESS;
   }
   if (NULL == dev_param_stack || NULL == dev_a_data || NULL == dev_b_data || NULL == dev_c_data) return EXIT_FAILURE;
+  if (xs_device_fault_pending()) return EXIT_FAILURE; /* a device error not yet cleared */
   result = xs_lazy_init();
   if (EXIT_SUCCESS != result) return result;
   xs_autotune_if_needed(m_max, n_max, k_max, stack_size, stream);
@@ -184,6 +188,7 @@ int libsmm_acc_transpose(const int* dev_trs_stack, int offset, int stack_size, v
   else if (dbcsr_type_real_4 == datatype) esize = 4;
   else return EXIT_SUCCESS;
   if (NULL == dev_trs_stack || NULL == dev_data) return EXIT_FAILURE;
+  if (xs_device_fault_pending()) return EXIT_FAILURE;
   result = xs_lazy_init();
   if (EXIT_SUCCESS != result) return result;
   return xs_record_error(xs_launch_transpose(dev_trs_stack, offset, stack_size, dev_data, esize, m, n,
@@ -236,6 +241,7 @@ int libxstream_b200_process_batch(const libxstream_b200_stack_t* stacks, int nst
     ++nonempty;
   }
   if (0 == nonempty) return EXIT_SUCCESS;
+  if (xs_device_fault_pending()) return EXIT_FAILURE;
   result = xs_lazy_init();
   if (EXIT_SUCCESS != result) return result;
   return xs_process_batch_part(stacks, nstacks, NULL != stream ? stream : xs_default_stream());

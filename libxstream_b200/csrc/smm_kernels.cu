@@ -615,7 +615,7 @@ __device__ __forceinline__ void drain_stage(uint64_t* bar, uint32_t parity) {
 template <int M_, int N_, int K_, int R>
 __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8))
   xs_smm_staged_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, unsigned* __restrict__ err,
-    unsigned* __restrict__ dev_err) {
+    unsigned* __restrict__ dev_err, long long wait_limit) {
   using G = Staged<M_, N_, K_>;
   constexpr int MT = G::MT, NT = G::NT, REGS = G::REGS, KS = G::KS;
   constexpr unsigned FULL = 0xFFFFFFFFu;
@@ -715,7 +715,8 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
       }
       const unsigned long long v = val_of(e);
       const int st = (e - p0) % R;
-      const bool ok = __all_sync(FULL, xs_tc::mbar_wait(&bar[st], (uint32_t)(((e - p0) / R) & 1), err, 2u) ? 1 : 0);
+      const bool ok =
+        __all_sync(FULL, xs_tc::mbar_wait(&bar[st], (uint32_t)(((e - p0) / R) & 1), err, 2u, wait_limit) ? 1 : 0);
       if (!ok) {
         bad = true;
         break;
@@ -1144,7 +1145,7 @@ cudaError_t launch_staged(const SmmPlan& pl, const StackTask& tk, int* seglist, 
   if (1 != pl.nsub) return cudaErrorInvalidValue; /* one warp tile per C block */
   void* prof = xs_profile_begin(s);
   r = pdl_launch(xs_smm_staged_kernel<M_, N_, K_, R>, pl.ngroups, 32 * pl.W, smem, s, tk, seglist, (unsigned*)err,
-    xs_device_error_ptr());
+    xs_device_error_ptr(), xs_wait_limit());
   if (cudaSuccess != r) return r;
   const double m = M_, n = N_, k = K_;
   xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);

@@ -9,7 +9,10 @@
  * synchronisation a growing pool or cudaFree can cause. For them, libxstream_b200_process_noalloc
  * runs the same kernels with the same results on a fixed scratch area that is part of the library
  * image: a file-scope device array of XS_NOALLOC_SCRATCH_BYTES (8 MiB) that every GPU on which the
- * library is used holds until the process exits. Nothing is allocated or freed per call.
+ * library is used holds until the process exits. Nothing is allocated or freed per call. Unlike
+ * libsmm_acc_process it does not pass stacks to an installed DBM launch hook and does not run the
+ * exhaustive autotuner (which allocates its own buffers): it uses the predicted or default
+ * parameters of a shape that was not tuned.
  *
  * Limits and rules:
  *   - a call whose stack needs more scratch than the array holds is rejected (nonzero return, a
@@ -41,9 +44,11 @@ static __device__ __align__(256) unsigned char xs_noalloc_scratch[XS_NOALLOC_SCR
 static pthread_mutex_t xs_noalloc_lock = PTHREAD_MUTEX_INITIALIZER;
 static void* xs_noalloc_addr[XS_NOALLOC_MAXDEV];
 
-/* Device address of the scratch array on the current device (looked up once per device). */
-static int xs_noalloc_scratch_address(int device, void** addr) {
-  int result = EXIT_SUCCESS;
+/* Device address of the scratch array on the calling thread's current CUDA device (looked up once
+   per device). cudaGetSymbolAddress resolves on that device, so the cache is indexed by it too. */
+static int xs_noalloc_scratch_address(void** addr) {
+  int result = EXIT_SUCCESS, device = -1;
+  if (cudaSuccess != cudaGetDevice(&device)) return xs_record_error((int)cudaGetLastError(), "cudaGetDevice");
   if (0 > device || XS_NOALLOC_MAXDEV <= device) return EXIT_FAILURE;
   pthread_mutex_lock(&xs_noalloc_lock);
   if (nullptr == xs_noalloc_addr[device]) {
@@ -84,6 +89,7 @@ int libxstream_b200_process_noalloc(const int* host_param_stack, const int* dev_
   if (nullptr == dev_param_stack || nullptr == dev_a_data || nullptr == dev_b_data || nullptr == dev_c_data) {
     return EXIT_FAILURE;
   }
+  if (xs_device_fault_pending()) return EXIT_FAILURE; /* a device error not yet cleared */
   result = xs_smm_ensure_init();
   if (EXIT_SUCCESS != result) return result;
   xs_params_lookup((int)datatype, m_max, n_max, k_max, stack_size, &prm);
@@ -95,7 +101,7 @@ int libxstream_b200_process_noalloc(const int* host_param_stack, const int* dev_
       stack_size, m_max, n_max, k_max, nbytes, XS_NOALLOC_SCRATCH_BYTES);
     return EXIT_FAILURE;
   }
-  result = xs_noalloc_scratch_address(xs_active_device(), &scratch);
+  result = xs_noalloc_scratch_address(&scratch);
   if (EXIT_SUCCESS != result) return result;
   return xs_record_error(xs_launch_smm_f64(dev_param_stack, stack_size, (const double*)dev_a_data,
                            (const double*)dev_b_data, (double*)dev_c_data, m_max, n_max, k_max, &prm, scratch,

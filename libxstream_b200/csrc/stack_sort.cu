@@ -844,14 +844,26 @@ unsigned* xs_device_error_ptr(void) {
   return addr[dev];
 }
 
+int xs_device_error_fetch(unsigned* host_dst, void* stream) {
+  unsigned* const p = xs_device_error_ptr();
+  if (nullptr == p) return (int)cudaErrorInvalidSymbol;
+  return (int)cudaMemcpyAsync(host_dst, p, sizeof(unsigned), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+}
+
+int xs_device_error_read(unsigned* value) {
+  return (int)cudaMemcpyFromSymbol(value, xs_device_error_word, sizeof(unsigned));
+}
+
+int xs_device_error_clear(void) {
+  const unsigned zero = 0;
+  return (int)cudaMemcpyToSymbol(xs_device_error_word, &zero, sizeof(zero));
+}
+
 int libxstream_b200_device_error(int reset) {
   unsigned e = 0;
   if (EXIT_SUCCESS != xs_ensure_device()) return -1;
-  if (cudaSuccess != cudaMemcpyFromSymbol(&e, xs_device_error_word, sizeof(e))) return -1;
-  if (0 != reset && 0 != e) {
-    const unsigned zero = 0;
-    if (cudaSuccess != cudaMemcpyToSymbol(xs_device_error_word, &zero, sizeof(zero))) return -1;
-  }
+  if (cudaSuccess != xs_device_error_read(&e)) return -1;
+  if (0 != reset && 0 != e && cudaSuccess != xs_device_error_clear()) return -1;
   return (int)e;
 }
 

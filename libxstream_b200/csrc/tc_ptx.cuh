@@ -49,14 +49,37 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return 0 != ok;
 }
 
+/* Non-blocking test of the phase with the given parity. */
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\t"
+    "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}"
+    : "=r"(ok)
+    : "r"(smem_u32(bar)), "r"(parity)
+    : "memory");
+  return 0 != ok;
+}
+
+/* Default bound of a pipeline wait in clock cycles (about two seconds at the boost clock); the
+   host may set another one per launch (libxstream_b200_set_wait_limit). */
+constexpr long long kDefaultWaitLimit = 4000000000ll;
+
 /* Waits for the phase with the given parity to complete. Gives up when *abort becomes non-zero
    (another role failed) or after `limit` clock cycles, then sets bit `code` in *abort and returns
    false; every wait of a kernel is bounded this way, so a protocol error ends the kernel with an
-   error status instead of a hang. */
+   error status instead of a hang. The first test does not block and the limit is checked right
+   after it, so a phase that is still pending when a wait with a limit of a few cycles starts always
+   gives up (the wait-limit test relies on that); later tests use the suspending try_wait. */
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* abort, unsigned code,
-  long long limit = 4000000000ll) {
-  if (mbar_try_wait(bar, parity)) return true;
+  long long limit = kDefaultWaitLimit) {
   const long long t0 = clock64();
+  if (mbar_test_wait(bar, parity)) return true;
+  if (clock64() - t0 > limit) {
+    atomicOr(abort, code);
+    return false;
+  }
   for (unsigned it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if (0 == (it & 63)) {

@@ -35,6 +35,8 @@ def lib() -> ctypes.CDLL:
         _lib.oracle_block_relerr.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int]
         _lib.oracle_block_relerr.restype = ctypes.c_double
         _lib.oracle_max_threads.restype = ctypes.c_int
+        _lib.oracle_fast_balance.argtypes = [ctypes.c_int, ctypes.c_int]
+        _lib.oracle_fast_balance.restype = ctypes.c_double
         _lib.oracle_ozaki_slice.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_byte), _ip]
         _lib.oracle_ozaki_gemm.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -67,7 +69,9 @@ def smm(stack: np.ndarray, a: np.ndarray, b: np.ndarray, c: np.ndarray, m: int, 
 
 def smm_fast(stack: np.ndarray, a: np.ndarray, b: np.ndarray, c: np.ndarray, m: int, n: int, k: int,
              threads: int = 0) -> np.ndarray:
-    """Timed CPU baseline (register-tiled, FMA, all threads; B column-major): C += A*B in place."""
+    """Timed CPU baseline (register-tiled, FMA, all threads; B column-major): C += A*B in place. The
+    stack is grouped by C and cut into equal contiguous ranges, one per thread (balanced whatever the
+    C distribution)."""
     stack = np.ascontiguousarray(stack, dtype=np.int32)
     assert a.dtype == b.dtype == c.dtype == np.float64 and c.flags.c_contiguous
     lib().oracle_smm_f64_fast(_p(stack, ctypes.c_int), stack.size // 3, _p(a, ctypes.c_double), _p(b, ctypes.c_double),
@@ -103,6 +107,11 @@ def max_threads() -> int:
     return int(lib().oracle_max_threads())
 
 
+def fast_balance(S: int, threads: int) -> float:
+    """Busiest thread's share of smm_fast's entries relative to the mean (1.0 = balanced)."""
+    return float(lib().oracle_fast_balance(int(S), int(threads)))
+
+
 def ozaki_slice(x: np.ndarray, rows: int, cols: int, rs: int, cs: int, nslices: int):
     """Digit planes int8[nslices, rows, cols] and per-row biased max exponent int32[rows]."""
     digits = np.zeros((nslices, rows, cols), dtype=np.int8)
@@ -129,5 +138,5 @@ def ozaki_smm(stack: np.ndarray, a: np.ndarray, b: np.ndarray, c: np.ndarray, m:
     return c
 
 
-__all__ = ["lib", "smm", "smm_fast", "transpose", "norms", "block_relerr", "max_threads", "ozaki_slice", "ozaki_gemm", "ozaki_smm", "OUT",
+__all__ = ["lib", "smm", "smm_fast", "fast_balance", "transpose", "norms", "block_relerr", "max_threads", "ozaki_slice", "ozaki_gemm", "ozaki_smm", "OUT",
            "Path"]

@@ -138,29 +138,119 @@ __attribute__((optimize("fp-contract=fast"))) static void smm_entry_fast(const d
   }
 }
 
-/* Timed CPU baseline: the host SMM path with all threads (B column-major). Thread t owns
-   the C blocks whose offset hashes to t, so each block is still updated in stack order by one
-   thread; results differ from oracle_smm_f64 only by FMA rounding. */
+/* Stable order of the stack by C offset (LSD radix sort of c - 1 in two 16-bit digits): perm[i] is
+   the stack index of the i-th entry in grouped order. Returns 0, or -1 if memory ran out. */
+static int group_by_c(const int* stack, int S, int* perm) {
+  int* const tmp = (int*)malloc(sizeof(int) * (size_t)(S > 0 ? S : 1));
+  size_t* const cnt = (size_t*)malloc(sizeof(size_t) * 65537);
+  int pass, i;
+  if (NULL == tmp || NULL == cnt) {
+    free(tmp);
+    free(cnt);
+    return -1;
+  }
+  for (i = 0; i < S; ++i) tmp[i] = i;
+  for (pass = 0; pass < 2; ++pass) {
+    const int sh = 16 * pass;
+    const int* const src = (0 == pass) ? tmp : perm;
+    int* const dst = (0 == pass) ? perm : tmp;
+    memset(cnt, 0, sizeof(size_t) * 65537);
+    for (i = 0; i < S; ++i) ++cnt[1 + ((((unsigned)stack[3 * src[i] + 2] - 1u) >> sh) & 0xFFFFu)];
+    for (i = 0; i < 65536; ++i) cnt[i + 1] += cnt[i];
+    for (i = 0; i < S; ++i) dst[cnt[(((unsigned)stack[3 * src[i] + 2] - 1u) >> sh) & 0xFFFFu]++] = src[i];
+  }
+  memcpy(perm, tmp, sizeof(int) * (size_t)S);
+  free(tmp);
+  free(cnt);
+  return 0;
+}
+
+/* Timed CPU baseline: the host SMM path with all threads (B column-major), balanced the way the
+   reference splits its host loop into tasks of equal length (libxs_gemm_index_task(..., tid, ntasks),
+   samples/smm/acc_bench.c:380-384). The stack is first ordered by C offset (stable), then cut into
+   nthreads contiguous ranges of equal entry count, so every thread does the same number of block
+   products whatever the C distribution (a Zipf-hot C block no longer lands on one thread). A
+   segment (run of equal C) inside a range is accumulated straight into C by its only owner; the
+   segments that cross a range boundary are accumulated into private partial tiles (head / tail of
+   each range), which are added to C afterwards in thread order, so the result is deterministic.
+   Results differ from oracle_smm_f64 only by rounding (FMA, and the partial sums). */
 void oracle_smm_f64_fast(const int* stack, int S, const double* a, const double* b, double* c, int m, int n, int k,
   int nthreads) {
+  const size_t mn = (size_t)m * n;
+  int* perm;
+  double* part;
+  int nt, t;
+  if (0 >= S) return;
 #if defined(_OPENMP)
   if (0 >= nthreads) nthreads = omp_get_max_threads();
-#pragma omp parallel num_threads(nthreads)
-  {
-    const int nt = omp_get_num_threads(), tid = omp_get_thread_num();
-    int s;
-    for (s = 0; s < S; ++s) {
-      const unsigned cblk = (unsigned)(stack[3 * s + 2] - 1) / (unsigned)(m * n);
-      if ((int)((cblk * 2654435761u) % (unsigned)nt) == tid) {
-        smm_entry_fast(a + stack[3 * s] - 1, b + stack[3 * s + 1] - 1, c + stack[3 * s + 2] - 1, m, n, k);
-      }
+#else
+  nthreads = 1;
+#endif
+  nt = (nthreads < S) ? nthreads : S;
+  if (0 >= nt) nt = 1;
+  perm = (int*)malloc(sizeof(int) * (size_t)S);
+  part = (double*)malloc(sizeof(double) * 2 * mn * (size_t)nt);
+  if (NULL == perm || NULL == part || 0 != group_by_c(stack, S, perm)) {
+    free(perm);
+    free(part);
+    return;
+  }
+#define XS_C_OF(I) (stack[3 * perm[I] + 2])
+#if defined(_OPENMP)
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+#endif
+  for (t = 0; t < nt; ++t) {
+    const int p0 = (int)((long long)S * t / nt), p1 = (int)((long long)S * (t + 1) / nt);
+    const int crossl = (0 < p0) && XS_C_OF(p0 - 1) == XS_C_OF(p0);
+    const int crossr = (p1 < S) && XS_C_OF(p1) == XS_C_OF(p1 - 1);
+    double* const head = part + 2 * mn * (size_t)t;
+    double* const tail = head + mn;
+    int q = p0;
+    memset(head, 0, sizeof(double) * 2 * mn);
+    while (q < p1) {
+      const int cq = XS_C_OF(q);
+      int r = q + 1, i;
+      double* dst;
+      while (r < p1 && XS_C_OF(r) == cq) ++r;
+      if (q == p0 && crossl) dst = head;       /* continues a segment of the previous range */
+      else if (r == p1 && crossr) dst = tail;  /* continues into the next range */
+      else dst = c + cq - 1;                   /* this thread's own C block */
+      for (i = q; i < r; ++i) smm_entry_fast(a + stack[3 * perm[i]] - 1, b + stack[3 * perm[i] + 1] - 1, dst, m, n, k);
+      q = r;
     }
   }
-#else
-  int s;
-  (void)nthreads;
-  for (s = 0; s < S; ++s) smm_entry_fast(a + stack[3 * s] - 1, b + stack[3 * s + 1] - 1, c + stack[3 * s + 2] - 1, m, n, k);
-#endif
+  for (t = 0; t < nt; ++t) { /* partial tiles of boundary-crossing segments, in thread order */
+    const int p0 = (int)((long long)S * t / nt), p1 = (int)((long long)S * (t + 1) / nt);
+    const int crossl = (0 < p0) && XS_C_OF(p0 - 1) == XS_C_OF(p0);
+    const int crossr = (p1 < S) && XS_C_OF(p1) == XS_C_OF(p1 - 1);
+    const int whole = crossl && XS_C_OF(p0) == XS_C_OF(p1 - 1); /* one segment spans the range: all in head */
+    const double* const head = part + 2 * mn * (size_t)t;
+    size_t e;
+    if (crossl) {
+      double* const dst = c + XS_C_OF(p0) - 1;
+      for (e = 0; e < mn; ++e) dst[e] += head[e];
+    }
+    if (crossr && !whole) {
+      double* const dst = c + XS_C_OF(p1 - 1) - 1;
+      for (e = 0; e < mn; ++e) dst[e] += head[mn + e];
+    }
+  }
+#undef XS_C_OF
+  free(perm);
+  free(part);
+}
+
+/* Largest share of the stack's entries that one thread of oracle_smm_f64_fast processes, relative to
+   the mean (1.0 = perfectly balanced). */
+double oracle_fast_balance(int S, int nthreads) {
+  int t, nt = (nthreads < S) ? nthreads : S;
+  long long most = 0;
+  if (0 >= nt) return 1.0;
+  for (t = 0; t < nt; ++t) {
+    const long long len = (long long)S * (t + 1) / nt - (long long)S * t / nt;
+    if (len > most) most = len;
+  }
+  return (double)most * nt / (double)S;
 }
 
 int oracle_max_threads(void) {

@@ -54,6 +54,21 @@ def test_timed_baseline_matches_checker(shape):
     assert oracle.block_relerr(fast, ref, m * n) < 1e-13
 
 
+@pytest.mark.parametrize("threads", [1, 3, 16, 64])
+def test_timed_baseline_balanced_on_zipf_stack(threads):
+    """The timed CPU baseline gives every thread the same number of entries even when one C block
+    takes ~18% of the stack (config 1's Zipf(1.1) c); boundary-crossing segments stay correct."""
+    case = W.config1()
+    m, n, k = case.m, case.n, case.k
+    assert oracle.fast_balance(case.S, threads) <= 1.1
+    sub = case.stack[: 3 * 6000]  # a prefix keeps the exact checker quick
+    ref = np.zeros(case.nc * m * n)
+    fast = np.zeros_like(ref)
+    oracle.smm(sub, case.a, case.b, ref, m, n, k, b_rowmajor=False)
+    oracle.smm_fast(sub, case.a, case.b, fast, m, n, k, threads=threads)
+    assert oracle.block_relerr(fast, ref, m * n) < 1e-13
+
+
 def test_oracle_transpose_numpy():
     g = W.rng(5)
     m, n = 7, 5
