@@ -188,10 +188,12 @@ int libxstream_b200_process_ozaki(const int* dev_param_stack, int stack_size, in
 /**
  * Exhaustive autotuner of the plain stack kernel (replaces samples/smm/tune_multiply.py's OpenTuner
  * search; the space here is the precompiled tile classes). libxstream_b200_tune_candidates writes
- * the (mt, nt, kp) triples tried for (m, n) and returns their count; libxstream_b200_tune times each
+ * the (mt, nt, kp) triples tried for (m, n) and returns their count (the DMMA tile classes, then
+ * (1, 1, -1), the register-blocked FMA kernel, where its lane grids cover m x n); libxstream_b200_tune times each
  * on synthetic data of the given shape and stack size (reps calls after one warm-up; seed fixes the
  * data) and, with ozaki_slices > 0 and m, n, k <= 64, the Ozaki form last; ms_out receives the
- * milliseconds per call. Returns the number of times written, < 0 on error. Synchronous.
+ * milliseconds per call (-1 for a candidate that does not take the shape). Returns the number of times
+ * written, < 0 on error. Synchronous.
  */
 int libxstream_b200_tune_candidates(int m, int n, int* mt_nt_kp, int capacity);
 int libxstream_b200_tune(int m, int n, int k, int stack_size, int reps, int ozaki_slices, unsigned seed, float* ms_out,

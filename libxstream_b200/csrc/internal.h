@@ -68,12 +68,15 @@ void xs_profile_end(void* token, const char* name, double flops, double bytes, v
 typedef struct xs_smm_params_t {
   int chunk;   /* entries per work item (L) */
   int mt, nt;  /* warp sub-tile, in units of 8x8 DMMA tiles (1..4 each) */
-  int kp;      /* k-steps (of 4) per register panel: 2 or 4 (1..4 for shape-specialised kernels) */
+  int kp;      /* k-steps (of 4) per register panel: 2 or 4 (1..4 for shape-specialised kernels); 0: staged
+                  kernel; XS_KP_FMA: register-blocked FMA kernel (no DMMA tiles) */
   int generic; /* 1: always use the runtime-shape kernel even if a specialised one exists */
   int wpb;     /* warps per CTA */
   int sorted;  /* 1: the stack is known to be grouped by c (skip the device sort) */
 } xs_smm_params_t;
 
+/** kp value that selects the register-blocked FMA stack kernel (small blocks). */
+#define XS_KP_FMA (-1)
 /** Where a lookup's parameters came from. */
 #define XS_PARAMS_DEFAULT 0   /* default heuristic */
 #define XS_PARAMS_TUNED 1     /* tuned record (table / CSV / autotuner) */
@@ -89,6 +92,9 @@ int xs_mlp_load_file(const char* path);
 /** Shape-specialised kernels compiled for (m, n, k): writes up to capacity (mt, nt, kp) triples,
     returns how many exist. */
 int xs_smm_f64_specialized(int m, int n, int k, int* mt_nt_kp, int capacity);
+
+/** 1 if the register-blocked FMA kernel takes blocks of m x n x k. */
+int xs_smm_fma_supported(int m, int n, int k);
 
 /** Size in bytes of the device scratch needed by xs_launch_smm_f64 for this call. */
 size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params);
@@ -170,6 +176,8 @@ typedef struct xs_sort_batch_t {
   int off[XS_MAX_BATCH];        /* first output position of each stack */
   int tile_begin[XS_MAX_BATCH]; /* filled by the launcher */
   int ntiles[XS_MAX_BATCH];     /* filled by the launcher */
+  unsigned blk[XS_MAX_BATCH];   /* > 0: the stack's C block size (its blocks do not overlap): bucket ids
+                                   floor((c - cmin) / blk), no gcd statistics; 0: gcd of the offsets */
   int* zero;                    /* nzero ints the grouping kernel sets to 0 before it ends (or nullptr) */
   int nzero;
 } xs_sort_batch_t;
@@ -190,10 +198,13 @@ int xs_stack_group_fits(const xs_sort_batch_t* desc);
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
 /** As xs_stack_group, for either parameter format; also zeroes nzero ints at zero (nullptr: none).
-    blk > 0: the C block size (blocks of the stack do not overlap), which spares the gcd statistics. */
+    blk > 0: the C block size (blocks of the stack do not overlap), which spares the gcd statistics.
+    heavy > 0: in a single-pass grouping (stacks of at most 32768 entries over at most 2048 block
+    positions), the C blocks with at least `heavy` entries come first, then the others, each class in
+    offset order (entries of one block stay in stack order). */
 int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
-  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
-  void* stream);
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, int heavy,
+  void* sort_scratch, void* stream);
 int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream);
 /** Device addresses inside the sort scratch: the work-queue counters of the stack kernels (one per

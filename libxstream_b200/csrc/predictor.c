@@ -99,19 +99,20 @@ static int xs_autotune_enabled(void) {
 
 void xs_autotune_if_needed(int m, int n, int k, int stack_size, void* stream) {
   xs_smm_params_t p;
-  int source = XS_PARAMS_DEFAULT, cand[3 * 32], nc, best = -1, i;
-  float ms[33];
+  int source = XS_PARAMS_DEFAULT, cand[3 * 33], nc, best = -1, i; /* 32 DMMA tile classes + the FMA kernel */
+  float ms[34];
   enum cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   cudaStream_t s = NULL;
   if (!xs_autotune_enabled()) return;
   xs_params_lookup_ex(3, m, n, k, stack_size, &p, &source);
   if (XS_PARAMS_TUNED == source || XS_PARAMS_PREDICTED == source) return;
   if (cudaSuccess != cudaStreamIsCapturing((cudaStream_t)stream, &cs) || cudaStreamCaptureStatusNone != cs) return;
-  nc = xs_tune_candidates(m, n, cand, 32);
+  nc = xs_tune_candidates(m, n, cand, 33);
+  if (nc > 33) return;
   if (cudaSuccess != cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) return;
-  if (nc == xs_tune(m, n, k, stack_size, 2, 0, 12345u, ms, 33, s)) {
-    for (i = 0; i < nc; ++i) {
-      if (0 > best || ms[i] < ms[best]) best = i;
+  if (nc == xs_tune(m, n, k, stack_size, 2, 0, 12345u, ms, 34, s)) {
+    for (i = 0; i < nc; ++i) { /* a negative time: the candidate does not take this shape */
+      if (0.f <= ms[i] && (0 > best || ms[i] < ms[best])) best = i;
     }
   }
   cudaStreamDestroy(s);

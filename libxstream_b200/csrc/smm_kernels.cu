@@ -57,6 +57,11 @@ cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, size_t sme
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+/* Release/acquire fence at GPU scope: orders this thread's piece stores before its (relaxed) arrival
+   increment, and a CTA's reads of the other CTAs' pieces after the increment that found them all
+   published. Lighter than the sequentially consistent __threadfence(). */
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 /* Bring a block of `count` contiguous doubles into L2 (one prefetch per 128-byte line, by 32 lanes). */
 __device__ __forceinline__ void prefetch_block_l2(const double* p, int count, int lane) {
   for (int x = 16 * lane; x < count + 15; x += 16 * 32) {
@@ -104,6 +109,16 @@ __device__ __forceinline__ void commit_tile(double* __restrict__ C, size_t coff,
   }
 }
 
+/* How a warp holds its C sub-tile, for the merge and combine code that sums pieces ([REGS][32]
+   doubles, element r of lane l at r * 32 + l) and writes a finished sum back: the DMMA fragments of an
+   8*MT x 8*NT sub-tile (element (i, j, h) at (i * NT + j) * 2 + h). */
+struct StackTask;
+template <int MT, int NT>
+struct DmmaLayout {
+  static constexpr int REGS = MT * NT * 2;
+  __device__ static __forceinline__ void commit(const StackTask& tk, int sub, size_t coff, const double (&sum)[REGS]);
+};
+
 /* Shared memory of the stack kernel: per warp two partial tiles (head / tail piece) + metadata. */
 template <int MT, int NT>
 __host__ __device__ constexpr size_t smm_smem_bytes(int warps) {
@@ -139,6 +154,22 @@ struct StackTask {
                      the stack kernel combines them itself; nullptr: they go to the combine kernel */
 };
 
+template <int MT, int NT>
+__device__ __forceinline__ void DmmaLayout<MT, NT>::commit(const StackTask& tk, int sub, size_t coff, const double (&sum)[REGS]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  double tile[MT][NT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      tile[i][j][0] = sum[(i * NT + j) * 2 + 0];
+      tile[i][j][1] = sum[(i * NT + j) * 2 + 1];
+    }
+  Tile<MT, NT> tl;
+  tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
+  commit_tile<MT, NT>(tk.c, coff, tile, tk.m, tk.n, g, t, tl, tk.alpha);
+}
+
 /* Segment-list entry: stack index (high 8 bits) and CTA group (low 24 bits). */
 __device__ __forceinline__ int seg_tag(int sid, int group) { return (sid << 24) | group; }
 
@@ -150,12 +181,13 @@ constexpr int kFan = 8;
 __device__ __forceinline__ int piece_slot(int j0, int q) { return (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q); }
 
 /* Groups j0 <= j <= j1 (j0, j1 returned) that hold entries of the segment with key x, for a segment
-   that the CTA group j holds and that crosses j's first boundary (head: entry j*Lc - 1 has key x)
+   that the CTA group j (W chunks of L entries, Lc = W*L) holds and that crosses j's first boundary
+   (head: entry j*Lc - 1 has key x)
    and/or its last one (tail: entry (j+1)*Lc has key x). Keys are sorted, so the boundaries a segment
    crosses are consecutive: one warp tests 32 boundaries per round (one load per lane). */
-__device__ __forceinline__ void segment_groups(const StackTask& tk, int j, unsigned x, bool head, bool tail, int& j0,
+__device__ __forceinline__ void segment_groups(const StackTask& tk, int W, int j, unsigned x, bool head, bool tail, int& j0,
   int& j1) {
-  const int lane = threadIdx.x & 31, Lc = tk.L * (blockDim.x >> 5);
+  const int lane = threadIdx.x & 31, Lc = tk.L * W;
   const unsigned* __restrict__ const keys = tk.keys;
   j0 = j;
   if (head) { /* boundary j - q (start of group j - q) is crossed iff entry (j - q) * Lc - 1 has key x */
@@ -183,6 +215,26 @@ __device__ __forceinline__ void segment_groups(const StackTask& tk, int j, unsig
   }
 }
 
+/* The CTA-level segment ranges of CTA group `group` (W chunks of L entries): probe[0] = the first
+   group holding the segment that enters the CTA (group if none enters), probe[1] = the last group
+   holding the segment that leaves it (group if none leaves). They depend on the grouped keys only, so
+   one warp computes them while the CTA's first copies are in flight, and the merge at the end does
+   not wait for these loads. Called by a whole warp; lane 0 writes probe. */
+__device__ __forceinline__ void probe_boundaries(const StackTask& tk, int W, int group, int* probe) {
+  const int S = tk.S, first = group * tk.L * W, lastp = min(first + tk.L * W, S) - 1;
+  const unsigned* __restrict__ const keys = tk.keys;
+  const unsigned k0 = keys[first], k1 = keys[lastp];
+  const bool hx = (0 < first) && keys[first - 1] == k0;
+  const bool tx = (lastp + 1 < S) && keys[lastp + 1] == k1;
+  int j0, j1, unused;
+  segment_groups(tk, W, group, k0, hx, false, j0, unused);
+  segment_groups(tk, W, group, k1, false, tx, unused, j1);
+  if (0 == (threadIdx.x & 31)) {
+    probe[0] = j0;
+    probe[1] = j1;
+  }
+}
+
 /* CTA-level merge of the warps' partial tiles. Chains start at warp 0's head piece (a segment
    entering the CTA) and at every tail piece (a segment starting in that warp's chunk); a chain
    continues through the head pieces of the following warps while the previous piece reaches the end
@@ -197,18 +249,19 @@ __device__ __forceinline__ void segment_groups(const StackTask& tk, int j, unsig
    and then arrives at the segment's counter) and the first-level sums at the end. The CTA records
    what it completed in duty[slot] = {1, j0, np, key, level, first-level group} for finish_segments.
    piece_at(w, slot) is warp w's head (slot 0) or tail (slot 1) piece in shared memory, [REGS][32]
-   doubles; meta[w][4] holds its head / head-spans / tail flags. Called by all threads after a CTA
-   barrier. */
-template <int MT, int NT, typename PieceAt>
+   doubles; meta[w][4] holds its head / head-spans / tail flags; probe (nullptr: found here) holds the
+   CTA's segment ranges from probe_boundaries. Called by all threads after a CTA barrier. */
+template <typename Lay, typename PieceAt>
 __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int sub, int* __restrict__ seglist,
-  const int* meta, int W, PieceAt piece_at, int (*duty)[6]) {
-  constexpr int REGS = MT * NT * 2;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int* meta, int W, PieceAt piece_at, int (*duty)[6], const int* probe = nullptr) {
+  constexpr int REGS = Lay::REGS;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int S = tk.S, L = tk.L, nchunks = tk.nchunks, nsub = tk.nsub;
   if (threadIdx.x < 12) duty[threadIdx.x / 6][threadIdx.x % 6] = 0;
   __syncthreads();
   for (int start = 0; start < 2; ++start) {
     const bool from_head = (0 == start);
+    if (warp >= W) break; /* warps beyond the W chunk owners (a producer warp) hold no pieces */
     if (from_head && 0 != warp) continue;
     if (0 == meta[warp * 4 + (from_head ? 0 : 2)]) continue;
     double sum[REGS];
@@ -240,16 +293,23 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
       }
       else {
         int j0, j1;
-        segment_groups(tk, group, key, from_head, spans, j0, j1);
+        if (nullptr != probe) { /* a head chain continues the segment entering the CTA; a spanning chain leaves it */
+          j0 = from_head ? probe[0] : group;
+          j1 = spans ? probe[1] : group;
+        }
+        else segment_groups(tk, W, group, key, from_head, spans, j0, j1);
         const int np = j1 - j0 + 1, q = group - j0;
         const int level = (np <= kFan) ? 2 : 1, i1 = q / kFan;
         const int target = (2 == level) ? np : min(kFan, np - i1 * kFan);
         int* const counter = (2 == level) ? tk.arrive + (size_t)j0 * nsub + sub
                                           : tk.arrive + (size_t)tk.ngroups * nsub + (size_t)piece_slot(j0, i1 * kFan) * nsub + sub;
-        __threadfence(); /* the piece is visible device-wide before the arrival */
+        fence_acq_rel_gpu(); /* the piece is visible device-wide before the arrival */
         __syncwarp();
         int last = 0;
-        if (0 == lane) last = (atomicAdd(counter, 1) == target - 1) ? 1 : 0;
+        if (0 == lane) {
+          last = (atomicAdd(counter, 1) == target - 1) ? 1 : 0;
+          if (last) fence_acq_rel_gpu(); /* acquire: the pieces this increment completed are visible */
+        }
         if (0 != __shfl_sync(0xFFFFFFFFu, last, 0) && 0 == lane) {
           int* const d = duty[from_head ? 0 : 1];
           d[1] = j0;
@@ -261,19 +321,7 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
         }
       }
     }
-    else {
-      double tile[MT][NT][2];
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-          tile[i][j][0] = sum[(i * NT + j) * 2 + 0];
-          tile[i][j][1] = sum[(i * NT + j) * 2 + 1];
-        }
-      Tile<MT, NT> tl;
-      tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
-      commit_tile<MT, NT>(tk.c, (size_t)key - 1, tile, tk.m, tk.n, g, t, tl, tk.alpha);
-    }
+    else Lay::commit(tk, sub, (size_t)key - 1, sum);
   }
 }
 
@@ -326,17 +374,17 @@ __device__ __forceinline__ void sum_pieces(const StackTask& tk, int sub, int cou
    the segment's counter; the CTA completing that counter (or a duty of a short segment) sums the
    segment's pieces or first-level sums in order and writes the block once. Called by all threads
    after a CTA barrier that follows cta_merge; ends with a barrier. */
-template <int MT, int NT>
+template <typename Lay>
 __device__ __forceinline__ void finish_segments(const StackTask& tk, int sub, int (*duty)[6], double* red) {
-  constexpr int REGS = MT * NT * 2;
+  constexpr int REGS = Lay::REGS;
   __shared__ int s_go;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nsub = tk.nsub;
   for (int d = 0; d < 2; ++d) {
     if (0 == duty[d][0]) continue; /* uniform: shared memory read after a barrier */
     const int j0 = duty[d][1], np = duty[d][2], level = duty[d][4], i1 = duty[d][5];
     const unsigned key = (unsigned)duty[d][3];
-    __threadfence(); /* the other CTAs published their pieces before their arrivals */
+    fence_acq_rel_gpu(); /* the other CTAs published their pieces before their arrivals */
     double acc[REGS];
     int count = np, stride = 1; /* what the final sum covers: pieces 0, stride, 2 * stride, ... */
     if (1 == level) {
@@ -346,34 +394,25 @@ __device__ __forceinline__ void finish_segments(const StackTask& tk, int sub, in
         double* const dst = tk.pieces + ((size_t)piece_slot(j0, q1) * nsub + sub) * REGS * 32 + lane;
 #pragma unroll
         for (int r = 0; r < REGS; ++r) __stcg(dst + r * 32, acc[r]);
-        __threadfence();
+        fence_acq_rel_gpu();
         __syncwarp();
         int last = 0;
-        if (0 == lane) last = (atomicAdd(tk.arrive + (size_t)j0 * nsub + sub, 1) == (np + kFan - 1) / kFan - 1) ? 1 : 0;
-        if (0 == lane) s_go = last;
+        if (0 == lane) {
+          last = (atomicAdd(tk.arrive + (size_t)j0 * nsub + sub, 1) == (np + kFan - 1) / kFan - 1) ? 1 : 0;
+          if (last) fence_acq_rel_gpu();
+          s_go = last;
+        }
       }
       __syncthreads();
       const int go = s_go;
       __syncthreads(); /* red and s_go may be reused */
       if (!go) continue;
-      __threadfence();
+      fence_acq_rel_gpu();
       count = (np + kFan - 1) / kFan;
       stride = kFan;
     }
     sum_pieces<REGS>(tk, sub, count, [&](int i) { return piece_slot(j0, i * stride); }, red, acc);
-    if (0 == warp) {
-      Tile<MT, NT> tl;
-      tl.init(sub, tk.nsub_n, tk.m, tk.n, g);
-      double tile[MT][NT][2];
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-          tile[i][j][0] = acc[(i * NT + j) * 2 + 0];
-          tile[i][j][1] = acc[(i * NT + j) * 2 + 1];
-        }
-      commit_tile<MT, NT>(tk.c, (size_t)key - 1, tile, tk.m, tk.n, g, t, tl, tk.alpha);
-    }
+    if (0 == warp) Lay::commit(tk, sub, (size_t)key - 1, acc);
     __syncthreads();
   }
 }
@@ -530,10 +569,10 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
   }
   __syncthreads();
   __shared__ int duty[2][6];
-  cta_merge<MT, NT>(tk, group, sub, seglist, meta, W,
+  cta_merge<DmmaLayout<MT, NT>>(tk, group, sub, seglist, meta, W,
     [&](int w, int slot) -> const double* { return sp + ((size_t)(w * 2 + slot) * REGS) * 32; }, duty);
   __syncthreads();
-  if (nullptr != tk.arrive) finish_segments<MT, NT>(tk, sub, duty, sp);
+  if (nullptr != tk.arrive) finish_segments<DmmaLayout<MT, NT>>(tk, sub, duty, sp);
 }
 
 template <int M_, int N_, int K_, int MT, int NT, int KP>
@@ -620,6 +659,7 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
   constexpr int MT = G::MT, NT = G::NT, REGS = G::REGS, KS = G::KS;
   constexpr unsigned FULL = 0xFFFFFFFFu;
   extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ int s_probe[2];
   pdl_wait();
   pdl_trigger();
   if (0 != *(volatile const unsigned*)err) return;
@@ -695,6 +735,7 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
       }
     };
     for (int q = 0; q < R - 1 && p0 + q < p1; ++q) issue(p0 + q, val_of(p0 + q));
+    if (0 == warp && nullptr != tk.arrive) probe_boundaries(tk, W, group, s_probe);
     int issued = min(R - 1, p1 - p0), segstart = p0, e = p0;
     unsigned key_cur = key_of(p0);
     for (; e < p1; ++e) {
@@ -821,13 +862,503 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
     return;
   }
   __shared__ int duty[2][6];
-  cta_merge<MT, NT>(tk, group, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
+  cta_merge<DmmaLayout<MT, NT>>(tk, group, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
+    return (const double*)(smraw + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
+  }, duty, (nullptr != tk.arrive && group * W < tk.nchunks) ? s_probe : nullptr);
+  if (nullptr != tk.arrive) {
+    __syncthreads();
+    finish_segments<DmmaLayout<MT, NT>>(tk, 0, duty, (double*)smraw);
+  }
+}
+
+/* ------------------------------------ warp-specialised staged stack kernel (one producer warp) */
+
+/* Shared memory of the warp-specialised kernel: NC rings of R stages (Staged geometry), then a full
+   and an empty mbarrier per stage, the merge metadata [NC][4] and 256 bytes of slack. */
+template <int M_, int N_, int K_>
+__host__ __device__ constexpr size_t ws_smem_bytes(int NC, int R) {
+  return (size_t)NC * Staged<M_, N_, K_>::warp_bytes(R) + (size_t)2 * NC * R * sizeof(uint64_t) + (size_t)NC * 4 * sizeof(int) + 256;
+}
+
+/* The staged stack kernel with its copies taken off the compute warps: a CTA of NC consumer warps
+   (one chunk of L grouped entries each, the same segments, pieces and merge as the staged kernel)
+   and one producer warp, whose lane w streams the A and B blocks of consumer w's entries into w's
+   ring of R stages (cp.async.bulk of the 16-byte-aligned windows, completion counted in bytes on the
+   stage's full barrier) as soon as w releases a stage (one arrival on its empty barrier). A consumer
+   only waits for its stage, runs the DMMAs from shared memory and releases it; the producer keeps
+   the next entry's payload in a register, so an issue never waits for a global load. Every wait is
+   bounded: a timed-out wait sets the grouping error word (which the other roles and CTAs poll), the
+   producer stops issuing and waits (bounded) for the copies still in flight, and the kernel sets a
+   device error bit and returns without writing. */
+template <int M_, int N_, int K_, int NC, int R, int MINB>
+__global__ void __launch_bounds__(32 * (NC + 1), MINB)
+  xs_smm_ws_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, unsigned* __restrict__ err,
+    unsigned* __restrict__ dev_err, long long wait_limit) {
+  using G = Staged<M_, N_, K_>;
+  constexpr int MT = G::MT, NT = G::NT, REGS = G::REGS, KS = G::KS;
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int group = blockIdx.x;
+  uint64_t* const fullb = (uint64_t*)(smraw + (size_t)NC * G::warp_bytes(R));
+  uint64_t* const emptyb = fullb + NC * R;
+  int* const meta = (int*)(emptyb + NC * R); /* [NC][4]: head, head spans the chunk, tail, entries consumed */
+  if (warp < NC && 0 == lane) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      xs_tc::mbar_init(&fullb[warp * R + q], 1);
+      xs_tc::mbar_init(&emptyb[warp * R + q], 1);
+    }
+    xs_tc::fence_barrier_init();
+    meta[warp * 4 + 0] = 0;
+    meta[warp * 4 + 1] = 0;
+    meta[warp * 4 + 2] = 0;
+    meta[warp * 4 + 3] = 0;
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (__syncthreads_or((0 != *(volatile const unsigned*)err) ? 1 : 0)) return; /* the grouping failed: write nothing */
+  const double* __restrict__ const A = tk.a;
+  const double* __restrict__ const B = tk.b;
+  const unsigned* __restrict__ const keys = tk.keys;
+  const unsigned long long* __restrict__ const vals = tk.vals;
+  const int S = tk.S, L = tk.L;
+  bool bad = false;
+  int issued = 0; /* producer lane w: entries of chunk w whose copies were issued */
+  if (NC == warp) { /* ------------------------------------------------------------- producer */
+    const int chunk = group * NC + lane;
+    const int p0 = chunk * L, n = (lane < NC && chunk < tk.nchunks) ? min(L, S - p0) : 0;
+    unsigned char* const ring = smraw + (size_t)lane * G::warp_bytes(R);
+    unsigned long long vnext = (0 < n) ? vals[p0] : 0ull;
+    long long t_prog = clock64();
+    while (__any_sync(FULL, issued < n)) {
+      bool ready = false;
+      if (issued < n) {
+        ready = (issued < R) || xs_tc::mbar_test_wait(&emptyb[lane * R + issued % R], (uint32_t)((issued / R - 1) & 1));
+      }
+      if (ready) {
+        const unsigned long long v = vnext;
+        if (issued + 1 < n) vnext = vals[p0 + issued + 1];
+        const int st = issued % R;
+        unsigned char* const dst = ring + st * G::STAGE;
+        const uintptr_t as = (uintptr_t)(A + ((unsigned)v - 1u)), bs = (uintptr_t)(B + ((unsigned)(v >> 32) - 1u));
+        const uintptr_t a0 = as & ~(uintptr_t)15, a1 = (as + (uintptr_t)M_ * K_ * 8 + 15) & ~(uintptr_t)15;
+        const uintptr_t b0 = bs & ~(uintptr_t)15, b1 = (bs + (uintptr_t)K_ * N_ * 8 + 15) & ~(uintptr_t)15;
+        uint64_t* const sb = &fullb[lane * R + st];
+        xs_tc::mbar_arrive_expect_tx(sb, (uint32_t)((a1 - a0) + (b1 - b0)));
+        xs_tc::bulk_load(dst, (const void*)a0, (uint32_t)(a1 - a0), sb);
+        xs_tc::bulk_load(dst + G::SA, (const void*)b0, (uint32_t)(b1 - b0), sb);
+        ++issued;
+      }
+      if (__any_sync(FULL, ready)) t_prog = clock64();
+      else { /* nobody released a stage: back off; give up on an abort or when the bound is passed */
+        if (0 != *(volatile const unsigned*)err) break;
+        if (clock64() - t_prog > wait_limit) {
+          if (0 == lane) atomicOr(err, 2u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  else { /* ------------------------------------------------------------------------ consumer */
+    unsigned char* const ring = smraw + (size_t)warp * G::warp_bytes(R);
+    const int chunk = group * NC + warp;
+    Tile<MT, NT> tl;
+    tl.init(0, 1, M_, N_, g);
+    const int lane_af = g + G::Q * M_ * t, lane_bf = g + G::Q * N_ * t;
+    const int lane_ar = g + G::QR * M_ * t, lane_br = g + G::QR * N_ * t;
+    double acc[MT][NT][2], hacc[MT][NT][2];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = hacc[i][j][0] = hacc[i][j][1] = 0.0;
+    int head = 0, hspans = 0, tail = 0, consumed = 0;
+    if (chunk < tk.nchunks) {
+      const int p0 = chunk * L, p1 = min(p0 + L, S);
+      const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
+      const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
+      int wb = p0;
+      unsigned kc = 0u, kn = 0u;
+      unsigned long long vc = 0ull, vn = 0ull;
+      if (p0 + lane < p1) {
+        kc = keys[p0 + lane];
+        vc = vals[p0 + lane];
+      }
+      if (p0 + 32 + lane < p1) {
+        kn = keys[p0 + 32 + lane];
+        vn = vals[p0 + 32 + lane];
+      }
+      auto key_of = [&](int e) -> unsigned {
+        const int i = e - wb;
+        const unsigned x0 = __shfl_sync(FULL, kc, i & 31), x1 = __shfl_sync(FULL, kn, i & 31);
+        return (i < 32) ? x0 : x1;
+      };
+      auto val_of = [&](int e) -> unsigned long long {
+        const int i = e - wb;
+        const unsigned long long x0 = __shfl_sync(FULL, vc, i & 31), x1 = __shfl_sync(FULL, vn, i & 31);
+        return (i < 32) ? x0 : x1;
+      };
+      int segstart = p0, e = p0;
+      unsigned key_cur = key_of(p0);
+      for (; e < p1; ++e) {
+        if (e - wb == 32) {
+          wb += 32;
+          kc = kn;
+          vc = vn;
+          kn = 0u;
+          vn = 0ull;
+          if (wb + 32 + lane < p1) {
+            kn = keys[wb + 32 + lane];
+            vn = vals[wb + 32 + lane];
+          }
+        }
+        const unsigned long long v = val_of(e);
+        const int st = (e - p0) % R;
+        const bool ok =
+          __all_sync(FULL, xs_tc::mbar_wait(&fullb[warp * R + st], (uint32_t)(((e - p0) / R) & 1), err, 2u, wait_limit) ? 1 : 0);
+        if (!ok) {
+          bad = true;
+          break;
+        }
+        const double* const sA = (const double*)(ring + st * G::STAGE) + (((uintptr_t)(A + ((unsigned)v - 1u)) >> 3) & 1u);
+        const double* const sB =
+          (const double*)(ring + st * G::STAGE + G::SA) + (((uintptr_t)(B + ((unsigned)(v >> 32) - 1u)) >> 3) & 1u);
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+          double fa[MT], fb[NT];
+          if (ks < G::GQ) {
+            constexpr int Q = G::Q;
+            const int kk = 4 * Q * (ks / Q) + ks % Q;
+#pragma unroll
+            for (int i = 0; i < MT; ++i) fa[i] = sA[lane_af + kk * M_ + 8 * i];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) fb[j] = sB[lane_bf + kk * N_ + 8 * j];
+          }
+          else {
+            constexpr int QR = G::QR;
+            const int kk = 4 * G::GQ + ((1 == QR) ? 4 * (ks - G::GQ) : (ks - G::GQ));
+            const bool kin = kk + QR * t < K_;
+#pragma unroll
+            for (int i = 0; i < MT; ++i) fa[i] = kin ? sA[lane_ar + kk * M_ + 8 * i] : 0.0;
+#pragma unroll
+            for (int j = 0; j < NT; ++j) fb[j] = kin ? sB[lane_br + kk * N_ + 8 * j] : 0.0;
+          }
+#pragma unroll
+          for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], fa[i], fb[j]);
+        }
+        __syncwarp(); /* every lane's fragment reads of the stage are done: hand it back */
+        if (0 == lane) xs_tc::mbar_arrive(&emptyb[warp * R + st]);
+        ++consumed;
+        const bool last = (e + 1 == p1);
+        const unsigned key_nxt = key_of(last ? e : e + 1);
+        if (last || key_nxt != key_cur) {
+          const bool crossl = headcross && (segstart == p0);
+          const bool crossr = tailcross && last;
+          if (!crossl && !crossr) commit_tile<MT, NT>(tk.c, (size_t)key_cur - 1, acc, M_, N_, g, t, tl, tk.alpha);
+          else if (!crossr) {
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+              for (int j = 0; j < NT; ++j) {
+                hacc[i][j][0] = acc[i][j][0];
+                hacc[i][j][1] = acc[i][j][1];
+              }
+            head = 1;
+          }
+          else if (crossl) {
+            head = 1;
+            hspans = 1;
+          }
+          else tail = 1;
+          if (!crossr) {
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+              for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+          }
+          segstart = e + 1;
+        }
+        key_cur = key_nxt;
+      }
+    }
+    __syncwarp();
+    if (0 == lane) meta[warp * 4 + 3] = consumed;
+    if (!bad) { /* every stage of this warp was consumed, so no copy is in flight: pieces go to its ring */
+      double* const sp = (double*)ring;
+      if (head) {
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) {
+            sp[((i * NT + j) * 2 + 0) * 32 + lane] = hspans ? acc[i][j][0] : hacc[i][j][0];
+            sp[((i * NT + j) * 2 + 1) * 32 + lane] = hspans ? acc[i][j][1] : hacc[i][j][1];
+          }
+      }
+      if (tail) {
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) {
+            sp[(REGS + (i * NT + j) * 2 + 0) * 32 + lane] = acc[i][j][0];
+            sp[(REGS + (i * NT + j) * 2 + 1) * 32 + lane] = acc[i][j][1];
+          }
+      }
+      if (0 == lane) {
+        meta[warp * 4 + 0] = head;
+        meta[warp * 4 + 1] = hspans;
+        meta[warp * 4 + 2] = tail;
+      }
+    }
+  }
+  if (__syncthreads_or((bad || (NC == warp && 0 != *(volatile const unsigned*)err)) ? 1 : 0)) {
+    /* the producer waits (bounded) for every copy it issued that its consumer did not take */
+    if (NC == warp && lane < NC) {
+      for (int q = meta[lane * 4 + 3]; q < issued; ++q) drain_stage(&fullb[lane * R + q % R], (uint32_t)((q / R) & 1));
+    }
+    if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
+    return;
+  }
+  __shared__ int duty[2][6];
+  cta_merge<DmmaLayout<MT, NT>>(tk, group, 0, seglist, meta, NC, [&](int w, int slot) -> const double* {
     return (const double*)(smraw + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
   }, duty);
   if (nullptr != tk.arrive) {
     __syncthreads();
-    finish_segments<MT, NT>(tk, 0, duty, (double*)smraw);
+    finish_segments<DmmaLayout<MT, NT>>(tk, 0, duty, (double*)smraw);
   }
+}
+
+/* ------------------------------------------------------ register-blocked FMA stack kernel (small blocks) */
+
+/* C layout of the FMA kernel: the 32 lanes form an LR x LC lane grid (LC = 32 / LR); lane (lr, lc),
+   lr = lane % LR, lc = lane / LR, holds the RB x CB elements in rows lr + LR*a (a < RB) and columns
+   lc*CB + b (b < CB) of C, element (a, b) at a*CB + b. Consecutive lanes hold consecutive rows, so
+   their A loads and C write-backs are contiguous; a lane's columns are contiguous, so its B loads
+   are pairs. */
+template <int LR, int RB, int CB>
+struct FmaLayout {
+  static constexpr int LC = 32 / LR;
+  static constexpr int REGS = RB * CB;
+  __device__ static __forceinline__ void commit(const StackTask& tk, int, size_t coff, const double (&sum)[REGS]) {
+    const int lane = threadIdx.x & 31, lr = lane % LR, lc = lane / LR, m = tk.m, n = tk.n;
+#pragma unroll
+    for (int a = 0; a < RB; ++a) {
+      const int row = lr + LR * a;
+      if (row < m) {
+#pragma unroll
+        for (int b = 0; b < CB; ++b) {
+          const int col = lc * CB + b;
+          if (col < n) atomicAdd(tk.c + coff + (size_t)col * m + row, tk.alpha * sum[a * CB + b]);
+        }
+      }
+    }
+  }
+};
+
+/* Shared memory of the FMA kernel, in doubles per warp: a ring of D stages, each the entry's A block
+   (m*k, column-major) rounded up to an even count followed by its B block (k*n, row-major); 32 doubles
+   of slack (reads of padding rows and columns pass the last stage by less than the slack); the head
+   piece [REGS][32]. The tail piece reuses the ring once it is drained. Then the merge metadata. The
+   slack is the lane grid's column count rounded up to even: a lane's B reads pass the end of a row
+   of n by at most LC*CB - n doubles. */
+__host__ __device__ constexpr int fma_stage(int m, int n, int k) { return ((m * k + 1) / 2 * 2 + k * n + 1) / 2 * 2; }
+__host__ __device__ constexpr int fma_ring(int m, int n, int k, int D, int regs, int slack) {
+  return (D * fma_stage(m, n, k) + slack > regs * 32) ? D * fma_stage(m, n, k) + slack : regs * 32;
+}
+__host__ __device__ constexpr size_t fma_smem_bytes(int m, int n, int k, int D, int regs, int slack, int W) {
+  return (size_t)W * (fma_ring(m, n, k, D, regs, slack) + regs * 32) * sizeof(double) + (size_t)W * 4 * sizeof(int);
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(xs_tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+/* The FMA stack kernel: the chunks, segments, pieces and merge of the other stack kernels, with C held
+   as FmaLayout<LR, RB, CB> register blocks and plain FP64 FMAs instead of padded DMMA tiles, so a
+   small or odd block (4^3, 5^3, 6x6x18, 13x4x16, 32x9x9, 16x64x9) issues no padding work. Each warp
+   streams the A and B blocks of the next D - 1 entries of its chunk into its ring with 8-byte
+   cp.async copies (lane l copies elements l, l + 32, ... of the entry's A | B window, one commit
+   group per entry), so D - 1 entries are in flight per warp without holding registers. Per k index a
+   lane reads RB values of A (a column of A: the lanes of one lane-grid column read consecutive rows)
+   and CB of B (one row of B, in pairs when the row length is even) and issues RB*CB FMAs. M_, N_, K_
+   > 0 fix the block shape at compile time; 0 means runtime (m <= LR*RB, n <= LC*CB). */
+template <int M_, int N_, int K_, int LR, int RB, int CB, int D>
+__global__ void __launch_bounds__(128, 2)
+  xs_smm_fma_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, const unsigned* __restrict__ err) {
+  using Lay = FmaLayout<LR, RB, CB>;
+  constexpr int REGS = Lay::REGS, SLACK = (Lay::LC * CB + 1) / 2 * 2;
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  extern __shared__ __align__(16) double fsm[];
+  __shared__ int s_probe[2];
+  pdl_wait();
+  pdl_trigger();
+  if (__syncthreads_or((0 != *(volatile const unsigned*)err) ? 1 : 0)) return;
+  const int m = M_ ? M_ : tk.m, n = N_ ? N_ : tk.n, k = K_ ? K_ : tk.k;
+  const int W = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lr = lane % LR, lc = lane / LR;
+  const int stage = fma_stage(m, n, k), sa = (m * k + 1) / 2 * 2, mk = m * k, tot = m * k + k * n;
+  const int region = fma_ring(m, n, k, D, REGS, SLACK) + REGS * 32;
+  double* const ring = fsm + (size_t)warp * region;
+  double* const hpiece = ring + fma_ring(m, n, k, D, REGS, SLACK);
+  int* const meta = (int*)(fsm + (size_t)W * region);
+  if (0 == lane) {
+    meta[warp * 4 + 0] = 0;
+    meta[warp * 4 + 1] = 0;
+    meta[warp * 4 + 2] = 0;
+  }
+  const double* __restrict__ const A = tk.a;
+  const double* __restrict__ const B = tk.b;
+  const unsigned* __restrict__ const keys = tk.keys;
+  const unsigned long long* __restrict__ const vals = tk.vals;
+  const int S = tk.S, L = tk.L;
+  const int chunk = blockIdx.x * W + warp;
+  double acc[REGS];
+#pragma unroll
+  for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
+  int head = 0, hspans = 0, tail = 0;
+  if (chunk < tk.nchunks) {
+    const int p0 = chunk * L, p1 = min(p0 + L, S);
+    const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
+    const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
+    int wb = p0;
+    unsigned kc = 0u, kn = 0u;
+    unsigned long long vc = 0ull, vn = 0ull;
+    if (p0 + lane < p1) {
+      kc = keys[p0 + lane];
+      vc = vals[p0 + lane];
+    }
+    if (p0 + 32 + lane < p1) {
+      kn = keys[p0 + 32 + lane];
+      vn = vals[p0 + 32 + lane];
+    }
+    auto key_of = [&](int e) -> unsigned {
+      const int i = e - wb;
+      const unsigned x0 = __shfl_sync(FULL, kc, i & 31), x1 = __shfl_sync(FULL, kn, i & 31);
+      return (i < 32) ? x0 : x1;
+    };
+    auto val_of = [&](int e) -> unsigned long long {
+      const int i = e - wb;
+      const unsigned long long x0 = __shfl_sync(FULL, vc, i & 31), x1 = __shfl_sync(FULL, vn, i & 31);
+      return (i < 32) ? x0 : x1;
+    };
+    /* copies of entry e's A | B window into its stage: lane l takes elements l, l + 32, ... */
+    auto issue = [&](int e, unsigned long long v) {
+      double* const dst = ring + ((e - p0) % D) * stage;
+      const double* const as = A + ((unsigned)v - 1u);
+      const double* const bs = B + ((unsigned)(v >> 32) - 1u);
+      for (int x = lane; x < tot; x += 32) {
+        if (x < mk) cp_async8(dst + x, as + x);
+        else cp_async8(dst + sa + (x - mk), bs + (x - mk));
+      }
+    };
+    for (int q = 0; q < D - 1; ++q) {
+      if (p0 + q < p1) issue(p0 + q, val_of(p0 + q));
+      cp_async_commit();
+    }
+    if (0 == warp) probe_boundaries(tk, W, blockIdx.x, s_probe);
+    int segstart = p0;
+    unsigned key_cur = key_of(p0);
+    for (int e = p0; e < p1; ++e) {
+      if (e - wb == 32) {
+        wb += 32;
+        kc = kn;
+        vc = vn;
+        kn = 0u;
+        vn = 0ull;
+        if (wb + 32 + lane < p1) {
+          kn = keys[wb + 32 + lane];
+          vn = vals[wb + 32 + lane];
+        }
+      }
+      cp_async_wait<D - 2>(); /* entry e's group has landed (this lane's copies) */
+      __syncwarp();           /* ... and every lane's; all lanes are done with entry e - 1's stage */
+      if (e + D - 1 < p1) issue(e + D - 1, val_of(e + D - 1));
+      cp_async_commit();
+      const double* const sA = ring + ((e - p0) % D) * stage;
+      const double* const sB = sA + sa;
+      auto fma_k = [&](int kk) {
+        double fa[RB], fb[CB];
+#pragma unroll
+        for (int a = 0; a < RB; ++a) fa[a] = sA[kk * m + lr + LR * a];
+        const double* const brow = sB + kk * n + lc * CB;
+        if (0 == (CB & 1) && 0 == (n & 1)) { /* 16-byte aligned pairs: the stage and B part start even */
+#pragma unroll
+          for (int b = 0; b < CB; b += 2) {
+            const double2 x = *(const double2*)(brow + b);
+            fb[b] = x.x;
+            fb[b + 1] = x.y;
+          }
+        }
+        else {
+#pragma unroll
+          for (int b = 0; b < CB; ++b) fb[b] = brow[b];
+        }
+#pragma unroll
+        for (int a = 0; a < RB; ++a)
+#pragma unroll
+          for (int b = 0; b < CB; ++b) acc[a * CB + b] = fma(fa[a], fb[b], acc[a * CB + b]);
+      };
+      if (0 < K_) {
+#pragma unroll
+        for (int kk = 0; kk < K_; ++kk) fma_k(kk);
+      }
+      else {
+        for (int kk = 0; kk < k; ++kk) fma_k(kk);
+      }
+      const bool last = (e + 1 == p1);
+      const unsigned key_nxt = key_of(last ? e : e + 1);
+      if (last || key_nxt != key_cur) { /* the segment ends with entry e */
+        const bool crossl = headcross && (segstart == p0);
+        const bool crossr = tailcross && last;
+        if (!crossl && !crossr) Lay::commit(tk, 0, (size_t)key_cur - 1, acc);
+        else if (!crossr) { /* continues the previous chunk's segment: head piece */
+#pragma unroll
+          for (int r = 0; r < REGS; ++r) hpiece[r * 32 + lane] = acc[r];
+          head = 1;
+        }
+        else if (crossl) { /* the whole chunk is one segment crossing both ends */
+          head = 1;
+          hspans = 1;
+        }
+        else tail = 1;
+        if (!crossr) {
+#pragma unroll
+          for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
+        }
+        segstart = e + 1;
+      }
+      key_cur = key_nxt;
+    }
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  if (hspans) {
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) hpiece[r * 32 + lane] = acc[r];
+  }
+  if (tail) { /* the ring is drained: the tail piece goes to its start */
+#pragma unroll
+    for (int r = 0; r < REGS; ++r) ring[r * 32 + lane] = acc[r];
+  }
+  if (0 == lane) {
+    meta[warp * 4 + 0] = head;
+    meta[warp * 4 + 1] = hspans;
+    meta[warp * 4 + 2] = tail;
+  }
+  __syncthreads();
+  __shared__ int duty[2][6];
+  cta_merge<Lay>(tk, blockIdx.x, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
+    const double* const base = fsm + (size_t)w * region;
+    return (0 == slot) ? base + fma_ring(m, n, k, D, REGS, SLACK) : base;
+  }, duty, s_probe);
+  __syncthreads();
+  finish_segments<Lay>(tk, 0, duty, fsm);
 }
 
 /* Task table of a batch (kernel parameter: read through the constant bank). */
@@ -1050,6 +1581,9 @@ typedef cudaError_t (*launch_fn_t)(const SmmPlan& pl, const StackTask& tk, int* 
   cudaStream_t s, int* occ);
 
 launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm);
+struct WsEntry;
+const WsEntry* find_ws(int m, int n, int k, int wpb);
+int fma_piece_regs(int m, int n, int k);
 
 /* Work decomposition and scratch layout of one call. An open chunk length (prm->chunk <= 0) is
    sized so that the grid is one full wave of resident CTAs: L = ceil(S * nsub / (resident * W)). */
@@ -1059,12 +1593,19 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   pl->no_combine = 0;
   pl->nsub_m = ((m + 7) / 8 + mt - 1) / mt;
   pl->nsub_n = ((n + 7) / 8 + nt - 1) / nt;
+  if (XS_KP_FMA == prm->kp) pl->nsub_m = pl->nsub_n = 1; /* the FMA lane grid covers the whole block */
   pl->nsub = pl->nsub_m * pl->nsub_n;
   pl->W = (prm->wpb >= 1 && prm->wpb <= 4) ? prm->wpb : 4;
+  if (0 == prm->generic && 4 < prm->wpb && nullptr != find_ws(m, n, k, prm->wpb) && (m + 7) / 8 == mt && (n + 7) / 8 == nt) {
+    pl->W = prm->wpb; /* warp-specialised kernel: wpb consumer warps, one chunk each */
+  }
   if (0 < prm->chunk) pl->L = prm->chunk;
   else {
     int occ = 0;
     StackTask none = {};
+    none.m = m; /* the shape sizes the shared memory of runtime-shape kernels */
+    none.n = n;
+    none.k = k;
     const launch_fn_t fn = find_launcher(m, n, k, prm);
     if (cudaSuccess != fn(*pl, none, nullptr, nullptr, 0, &occ) || occ < 1) occ = 1;
     const long resident = (long)occ * xs_sm_count();
@@ -1089,8 +1630,10 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
   off += vs;
   pl->off_seglist = off;
   off = align_up(off + sizeof(int) * ((size_t)pl->ngroups + 1), 256);
-  pl->off_pieces = off;
-  off = align_up(off + sizeof(double) * (size_t)2 * pl->ngroups * pl->nsub * (mt * nt * 2) * 32, 256);
+  pl->off_pieces = off; /* two pieces per CTA group and sub-tile, one warp's accumulators each */
+  const int regs = (XS_KP_FMA == prm->kp) ? fma_piece_regs(m, n, k) : mt * nt * 2;
+  if (0 >= regs) return -1;
+  off = align_up(off + sizeof(double) * (size_t)2 * pl->ngroups * pl->nsub * regs * 32, 256);
   pl->off_arrive = off; /* segment counters [ngroups][nsub], then first-level counters [2 ngroups][nsub] */
   off = align_up(off + sizeof(int) * (size_t)3 * pl->ngroups * pl->nsub, 256);
   pl->off_sort = off;
@@ -1152,6 +1695,88 @@ cudaError_t launch_staged(const SmmPlan& pl, const StackTask& tk, int* seglist, 
   return (pl.no_combine || nullptr != tk.arrive) ? cudaSuccess : launch_combine<G::MT, G::NT>(pl, tk, seglist, err, s);
 }
 
+/* The warp-specialised staged kernel of one block shape: NC consumer warps + one producer warp per
+   CTA, rings of R stages, MINB CTAs per SM; then the combine (when the stack kernel does not combine
+   its CTA-crossing segments itself). */
+template <int M_, int N_, int K_, int NC, int R, int MINB>
+cudaError_t launch_ws(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err, cudaStream_t s, int* occ) {
+  using G = Staged<M_, N_, K_>;
+  cudaError_t r;
+  const size_t smem = ws_smem_bytes<M_, N_, K_>(NC, R);
+  r = (cudaError_t)xs_func_smem((const void*)xs_smm_ws_kernel<M_, N_, K_, NC, R, MINB>, smem);
+  if (cudaSuccess != r) return r;
+  if (nullptr != occ) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_ws_kernel<M_, N_, K_, NC, R, MINB>, 32 * (NC + 1), smem);
+  }
+  if (1 != pl.nsub || NC != pl.W) return cudaErrorInvalidValue; /* one warp tile per C block, NC chunks per CTA */
+  void* prof = xs_profile_begin(s);
+  r = pdl_launch(xs_smm_ws_kernel<M_, N_, K_, NC, R, MINB>, pl.ngroups, 32 * (NC + 1), smem, s, tk, seglist, (unsigned*)err,
+    xs_device_error_ptr(), xs_wait_limit());
+  if (cudaSuccess != r) return r;
+  const double m = M_, n = N_, k = K_;
+  xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * (m * k + k * n + 2.0 * m * n), s);
+  return (pl.no_combine || nullptr != tk.arrive) ? cudaSuccess : launch_combine<G::MT, G::NT>(pl, tk, seglist, err, s);
+}
+
+/* The FMA kernel: FmaLayout<LR, RB, CB> tiles, D-deep cp.async ring per warp. Its CTA-crossing segments
+   are combined inside the kernel (the combine kernel takes DMMA-layout pieces only). */
+template <int M_, int N_, int K_, int LR, int RB, int CB, int D>
+cudaError_t launch_fma(const SmmPlan& pl, const StackTask& tk, int* seglist, const unsigned* err, cudaStream_t s, int* occ) {
+  constexpr int REGS = RB * CB, SLACK = (32 / LR * CB + 1) / 2 * 2;
+  const int m = M_ ? M_ : tk.m, n = N_ ? N_ : tk.n, k = K_ ? K_ : tk.k;
+  if (m < 1 || n < 1 || k < 1 || m > LR * RB || n > 32 / LR * CB) return cudaErrorInvalidValue;
+  const size_t smem = fma_smem_bytes(m, n, k, D, REGS, SLACK, pl.W);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t r = (cudaError_t)xs_func_smem((const void*)xs_smm_fma_kernel<M_, N_, K_, LR, RB, CB, D>, smem);
+  if (cudaSuccess != r) return r;
+  if (nullptr != occ) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, xs_smm_fma_kernel<M_, N_, K_, LR, RB, CB, D>, 32 * pl.W, smem);
+  }
+  if (1 != pl.nsub || nullptr == tk.arrive) return cudaErrorInvalidValue;
+  void* prof = xs_profile_begin(s);
+  r = pdl_launch(xs_smm_fma_kernel<M_, N_, K_, LR, RB, CB, D>, pl.ngroups, 32 * pl.W, smem, s, tk, seglist, err);
+  if (cudaSuccess != r) return r;
+  xs_profile_end(prof, "smm", 2.0 * m * n * k * (double)tk.S, 8.0 * tk.S * ((double)m * k + (double)k * n + 2.0 * m * n), s);
+  return cudaSuccess;
+}
+
+/* FMA kernels: shapes compiled with their own lane grids, then runtime-shape classes (k <= 80) for any
+   block whose C fits the class's lane grid; a shape takes the class with the fewest padded elements. */
+struct FmaEntry {
+  int m, n, k; /* 0: runtime */
+  int mmax, nmax;
+  int regs; /* accumulators per lane (RB * CB): the size of a piece is regs * 32 doubles */
+  launch_fn_t fn;
+};
+#define XS_FMA(M, N, K, LR, RB, CB, D) {M, N, K, M, N, RB * CB, &launch_fma<M, N, K, LR, RB, CB, D>}
+#define XS_FMA_RT(LR, RB, CB, D) {0, 0, 0, LR * RB, 32 / LR * CB, RB * CB, &launch_fma<0, 0, 0, LR, RB, CB, D>}
+static const FmaEntry fma_table[] = {
+  XS_FMA(4, 4, 4, 4, 1, 1, 8), XS_FMA(5, 5, 5, 8, 1, 2, 8), XS_FMA(6, 6, 18, 8, 1, 2, 6), XS_FMA(13, 4, 16, 16, 1, 2, 6),
+  XS_FMA(32, 9, 9, 16, 2, 5, 4), XS_FMA(16, 64, 9, 8, 2, 16, 3), XS_FMA(7, 10, 5, 8, 1, 3, 8),
+  XS_FMA_RT(8, 1, 1, 8), XS_FMA_RT(8, 1, 2, 8), XS_FMA_RT(8, 2, 2, 6), XS_FMA_RT(8, 2, 4, 6), XS_FMA_RT(16, 2, 4, 4),
+  XS_FMA_RT(16, 2, 8, 4), XS_FMA_RT(8, 2, 8, 4), XS_FMA_RT(8, 2, 16, 3), XS_FMA_RT(16, 2, 16, 3),
+};
+constexpr int kFmaMaxK = 80;
+
+const FmaEntry* find_fma(int m, int n, int k) {
+  const FmaEntry* best = nullptr;
+  for (const FmaEntry& e : fma_table) {
+    if (0 != e.m) {
+      if (e.m == m && e.n == n && e.k == k) return &e;
+      continue;
+    }
+    if (m > e.mmax || n > e.nmax || k > kFmaMaxK) continue;
+    if (nullptr == best || e.mmax * e.nmax < best->mmax * best->nmax) best = &e;
+  }
+  return best;
+}
+
+/* Accumulators per lane of the FMA kernel that runs (m, n, k), 0 if none does. */
+int fma_piece_regs(int m, int n, int k) {
+  const FmaEntry* const f = find_fma(m, n, k);
+  return (nullptr != f) ? f->regs : 0;
+}
+
 /* Runtime-shape kernels: any (m, n, k), warp sub-tile MT x NT, KP in {2, 4}. */
 #define XS_KP_ENTRY(MT, NT) {&launch_dmma<0, 0, 0, MT, NT, 2>, &launch_dmma<0, 0, 0, MT, NT, 4>}
 static const launch_fn_t launch_table[4][4][2] = {
@@ -1185,12 +1810,38 @@ static const SpecEntry staged_table[] = {
   XS_STAGED3(22, 32, 32, 2), XS_STAGED3(16, 64, 9, 2),
 };
 
+/* Shapes with a warp-specialised staged kernel, selected by the warps-per-CTA parameter (wpb = NC,
+   the consumer warps; values above 4, which the other kernels do not take). */
+struct WsEntry {
+  int m, n, k, nc;
+  launch_fn_t fn;
+};
+#define XS_WS(M, N, K, NC, R, MINB) {M, N, K, NC, &launch_ws<M, N, K, NC, R, MINB>}
+static const WsEntry ws_table[] = {
+  XS_WS(23, 23, 23, 12, 2, 1), XS_WS(23, 23, 23, 6, 2, 2), XS_WS(23, 23, 23, 8, 3, 1),
+};
+
+const WsEntry* find_ws(int m, int n, int k, int wpb) {
+  for (const WsEntry& e : ws_table) {
+    if (e.m == m && e.n == n && e.k == k && e.nc == wpb) return &e;
+  }
+  return nullptr;
+}
+
 cudaError_t launch_unsupported(const SmmPlan&, const StackTask&, int*, const unsigned*, cudaStream_t, int*) {
   return cudaErrorInvalidValue;
 }
 
 launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
+  if (XS_KP_FMA == prm->kp) {
+    const FmaEntry* const f = find_fma(m, n, k);
+    return (nullptr != f) ? f->fn : &launch_unsupported;
+  }
   if (0 == prm->generic) {
+    if (4 < prm->wpb) {
+      const WsEntry* const w = find_ws(m, n, k, prm->wpb);
+      if (nullptr != w && (m + 7) / 8 == prm->mt && (n + 7) / 8 == prm->nt) return w->fn;
+    }
     for (const SpecEntry& e : staged_table) {
       if (e.m == m && e.n == n && e.k == k && e.mt == prm->mt && e.nt == prm->nt) return e.fn;
     }
@@ -1301,6 +1952,7 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     if (0 >= st[i].stack_size) continue;
     xs_smm_params_t prm;
     xs_params_lookup(3, st[i].m, st[i].n, st[i].k, st[i].stack_size, &prm);
+    if (4 < prm.wpb) prm.wpb = kBatchW; /* batch parts run kBatchW chunks per CTA */
     for (int first = 0; first < st[i].stack_size; first += smax) {
       if (bp->nparts == kMaxBatchTasks) return -1;
       BatchPart& p = bp->part[bp->nparts++];
@@ -1325,15 +1977,24 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
   for (int q = 0; q < bp->nparts; ++q) {
     BatchPart& p = bp->part[q];
     const libxstream_b200_stack_t& d = st[p.stack];
-    const int nsub = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
+    const int nsub = (XS_KP_FMA == p.prm.kp) ? 1 : ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
     SmmPlan pl = {};
     pl.W = kBatchW;
     StackTask none = {};
+    none.m = d.m;
+    none.n = d.n;
+    none.k = d.k;
     int occ = 0;
     if (cudaSuccess != find_launcher(d.m, d.n, d.k, &p.prm)(pl, none, nullptr, nullptr, 0, &occ) || occ < 1) occ = 1;
     const long resident = (long)occ * xs_sm_count();
     solo_L[q] = (int)(((long)p.S * nsub + resident * kBatchW - 1) / (resident * kBatchW));
     p.solo = (solo_L[q] >= kSoloMinL) ? 1 : 0;
+    if (!p.solo && XS_KP_FMA == p.prm.kp) { /* the persistent kernels run DMMA tiles only */
+      xs_params_default(d.m, d.n, d.k, p.S, &p.prm);
+      if (0 == p.prm.kp) p.prm.kp = 2;
+      p.mt = p.prm.mt;
+      p.nt = p.prm.nt;
+    }
     if (!p.solo && (p.mt > 4 || p.nt > 4)) { /* the persistent kernels take tiles of up to 4 x 4 fragments */
       p.mt = p.prm.mt = min(p.mt, 4);
       p.nt = p.prm.nt = min(p.nt, 4);
@@ -1363,6 +2024,7 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     const libxstream_b200_stack_t& d = st[p.stack];
     bp->nsub_n[q] = (((d.n + 7) / 8) + p.nt - 1) / p.nt;
     bp->nsub[q] = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * bp->nsub_n[q];
+    if (XS_KP_FMA == p.prm.kp) bp->nsub_n[q] = bp->nsub[q] = 1; /* the FMA lane grid covers the block */
     const double per_entry = p.mt * p.nt * ((d.k + 3) / 4) + 8;
     long L = p.solo ? solo_L[q] : (long)(target[batch_group(p.mt, p.nt)] / (kBatchW * per_entry) + 0.5);
     if (L < 1) L = 1;
@@ -1374,7 +2036,9 @@ int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
     bp->off_part[q] = off;
     off += (size_t)p.S;
     bp->pieces_off[q] = poff;
-    poff += (size_t)2 * bp->ngroups[q] * bp->nsub[q] * (p.mt * p.nt * 2) * 32;
+    const int regs = (XS_KP_FMA == p.prm.kp) ? fma_piece_regs(d.m, d.n, d.k) : p.mt * p.nt * 2;
+    if (0 >= regs) return -1;
+    poff += (size_t)2 * bp->ngroups[q] * bp->nsub[q] * regs * 32;
     bp->arrive_off[q] = narrive;
     if (p.solo) narrive += (size_t)3 * bp->ngroups[q] * bp->nsub[q];
     bp->ngroups_total += bp->ngroups[q];
@@ -1554,6 +2218,19 @@ int xs_smm_f64_specialized(int m, int n, int k, int* mt_kp_pairs, int capacity) 
   return count;
 }
 
+int xs_smm_fma_supported(int m, int n, int k) {
+  const FmaEntry* const f = find_fma(m, n, k);
+  if (nullptr == f) return 0;
+  int occ = 0; /* the lane grid covers the block; the ring of the shape must also fit shared memory */
+  SmmPlan pl = {};
+  pl.W = 4;
+  StackTask tk = {};
+  tk.m = m;
+  tk.n = n;
+  tk.k = k;
+  return (cudaSuccess == f->fn(pl, tk, nullptr, nullptr, 0, &occ) && 0 < occ) ? 1 : 0;
+}
+
 size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params) {
   SmmPlan pl;
   if (stack_size > xs_stack_group_max()) stack_size = xs_stack_group_max(); /* processed in parts */
@@ -1593,7 +2270,7 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   int* const arrive = (int*)(base + pl.off_arrive);
   void* prof = xs_profile_begin(s);
   const int r = xs_stack_group_ex(dev_stack, S, format, (unsigned)(m * n), keys_in, vals_in, keys_tmp, vals_tmp, keys_out,
-    vals_out, seglist, arrive, 3 * pl.ngroups * pl.nsub, sort_scratch, s);
+    vals_out, seglist, arrive, 3 * pl.ngroups * pl.nsub, pl.L * pl.W, sort_scratch, s);
   if (0 != r) return r;
   xs_profile_end(prof, "sort", 0.0, 48.0 * S, s);
   StackTask tk = {};
@@ -1672,6 +2349,7 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     sb.format[sb.nstacks] = 0;
     sb.S[sb.nstacks] = p.S;
     sb.off[sb.nstacks] = (int)bp.off_part[q];
+    sb.blk[sb.nstacks] = (unsigned)(st[p.stack].m * st[p.stack].n);
     ++sb.nstacks;
     tiles += nt;
   }

@@ -38,9 +38,9 @@ static void xs_sanitize(xs_smm_params_t* p) {
   p->chunk = xs_clamp(p->chunk, 0, 1 << 20); /* 0: sized per stack by the launcher */
   p->mt = xs_clamp(p->mt, 1, 4);
   p->nt = xs_clamp(p->nt, 1, 4);
-  p->kp = xs_clamp(p->kp, 0, 4); /* 0: staged kernel (where compiled for the shape) */
+  p->kp = xs_clamp(p->kp, XS_KP_FMA, 4); /* 0: staged kernel (where compiled for the shape); -1: FMA kernel */
   p->generic = (0 != p->generic) ? 1 : 0;
-  p->wpb = xs_clamp(p->wpb, 1, 4);
+  p->wpb = xs_clamp(p->wpb, 1, 16); /* above 4: consumer warps of a warp-specialised kernel */
   p->sorted = (0 != p->sorted) ? 1 : 0;
 }
 

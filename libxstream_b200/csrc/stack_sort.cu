@@ -72,37 +72,34 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-/* Bounded grid barrier (all CTAs are co-resident: cooperative launch). Returns false on timeout
-   or if another CTA reported an error. */
-__device__ bool grid_sync(SortCtl* ctl) {
+/* Bounded grid barrier (all CTAs are co-resident: cooperative launch). The arrival counter only
+   grows (it is zeroed with the control block at the start of the call): barrier number `epoch`
+   (0, 1, ...) of the launch is passed once it reaches (epoch + 1) * gridDim.x, so the last CTA to
+   arrive resets nothing and the others leave on their next poll. Returns false on timeout or if
+   another CTA reported an error. */
+__device__ __forceinline__ bool grid_sync(SortCtl* ctl, int& epoch) {
   __shared__ int s_ok;
   __syncthreads();
   if (0 == threadIdx.x) {
-    volatile unsigned* const vgen = &ctl->bar_gen;
-    const unsigned gen = *vgen;
+    const unsigned target = (unsigned)(epoch + 1) * gridDim.x;
     __threadfence();
-    const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
+    unsigned seen = atomicAdd(&ctl->bar_count, 1u) + 1u;
     int ok = 1;
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&ctl->bar_count, 0u);
-      __threadfence();
-      atomicAdd(&ctl->bar_gen, 1u);
-    }
-    else {
-      unsigned spins = 0;
-      while (*vgen == gen) {
-        if (++spins > kSpinLimit) {
-          atomicExch(&ctl->err, 1u);
-          atomicOr(&xs_device_error_word, 1u);
-          ok = 0;
-          break;
-        }
+    unsigned spins = 0;
+    while (seen < target) {
+      if (++spins > kSpinLimit) {
+        atomicExch(&ctl->err, 1u);
+        atomicOr(&xs_device_error_word, 1u);
+        ok = 0;
+        break;
       }
+      seen = *(volatile unsigned*)&ctl->bar_count;
     }
     __threadfence();
     if (0 != *(volatile unsigned*)&ctl->err) ok = 0;
     s_ok = ok;
   }
+  ++epoch;
   __syncthreads();
   return 0 != s_ok;
 }
@@ -113,9 +110,19 @@ __device__ __forceinline__ unsigned bucket_of(unsigned c, unsigned cmin, double 
   return __double2uint_rn((double)(c - cmin) * inv_g);
 }
 
-/* Block-wide exclusive scan of R values held PER per thread (thread i owns [i*PER, (i+1)*PER)). */
+/* floor(x / d) for d >= 1 from m = floor(2^32 / d) (m = 0 for d = 1): the high product is q or
+   q - 1, one correction step fixes it. */
+__device__ __forceinline__ unsigned div_floor(unsigned x, unsigned d, unsigned m) {
+  if (1u >= d) return x;
+  unsigned q = __umulhi(x, m);
+  if ((unsigned long long)(q + 1u) * d <= x) ++q;
+  return q;
+}
+
+/* Block-wide exclusive scan of R values held PER per thread (thread i owns [i*PER, (i+1)*PER));
+   returns the block total. */
 template <int PER>
-__device__ __forceinline__ void block_exscan(int (&v)[PER], int* s_wsum) {
+__device__ __forceinline__ int block_exscan(int (&v)[PER], int* s_wsum) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int sum = 0;
 #pragma unroll
@@ -128,8 +135,11 @@ __device__ __forceinline__ void block_exscan(int (&v)[PER], int* s_wsum) {
   }
   if (31 == lane) s_wsum[warp] = x;
   __syncthreads();
-  int run = x - sum;
-  for (int w2 = 0; w2 < warp; ++w2) run += s_wsum[w2];
+  int run = x - sum, total = 0;
+  for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) {
+    if (w2 < warp) run += s_wsum[w2];
+    total += s_wsum[w2];
+  }
 #pragma unroll
   for (int j = 0; j < PER; ++j) {
     const int t = v[j];
@@ -137,6 +147,7 @@ __device__ __forceinline__ void block_exscan(int (&v)[PER], int* s_wsum) {
     run += t;
   }
   __syncthreads();
+  return total;
 }
 
 /* Grouping sort of a batch of stacks. Tile t belongs to stack s with tile_begin[s] <= t <
@@ -150,26 +161,52 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
   unsigned long long* __restrict__ v0, unsigned* __restrict__ k1, unsigned long long* __restrict__ v1,
   unsigned* __restrict__ kout, unsigned long long* __restrict__ vout, int* __restrict__ seglist,
   int* __restrict__ hist, SortCtl* ctl, unsigned long long* __restrict__ stamps) {
-  __shared__ unsigned short s_wc[kSortWarps][kRadix];
+  __shared__ __align__(16) unsigned short s_wc[kSortWarps][kRadix]; /* (b) reuses it as int[kRadix] */
   __shared__ int s_base[kRadix]; /* digit histogram in (a), digit write positions in (b)/(c) */
   __shared__ int s_wsum[kSortWarps];
   __shared__ unsigned s_red[3][kSortWarps];
   __shared__ int s_radix[XS_MAX_BATCH]; /* digit range R of every stack of the batch */
-  const int tile = blockIdx.x, ntiles_all = gridDim.x;
+  /* per-stack tables of the descriptor, read with compile-time indices only (an index computed at
+     run time would make every thread copy the whole descriptor to local memory) */
+  __shared__ int s_tb[XS_MAX_BATCH], s_nt[XS_MAX_BATCH], s_gidx[XS_MAX_BATCH];
+  __shared__ unsigned s_blk[XS_MAX_BATCH];
+#pragma unroll
+  for (int s2 = 0; s2 < XS_MAX_BATCH; ++s2) {
+    if (s2 == (int)threadIdx.x) {
+      s_tb[s2] = desc.tile_begin[s2];
+      s_nt[s2] = desc.ntiles[s2];
+      s_gidx[s2] = desc.gidx[s2];
+      s_blk[s2] = desc.blk[s2];
+    }
+  }
+  __syncthreads();
+  const int tile = blockIdx.x, ntiles_all = gridDim.x, nstacks = desc.nstacks;
   int si = 0;
-  while (si + 1 < desc.nstacks && desc.tile_begin[si + 1] <= tile) ++si;
-  const int* const stack = desc.stack[si];
+  while (si + 1 < nstacks && s_tb[si + 1] <= tile) ++si;
+  const int* stack = nullptr;
+  int fmt = 0, S = 0, off = 0;
+#pragma unroll
+  for (int s2 = 0; s2 < XS_MAX_BATCH; ++s2) {
+    if (s2 == si) {
+      stack = desc.stack[s2];
+      fmt = desc.format[s2];
+      S = desc.S[s2];
+      off = desc.off[s2];
+    }
+  }
   /* parameter format: 1-based (a, b, c) triples, or 6-int records with 0-based (a, b, c) at +3 */
-  const int pstride = (0 != desc.format[si]) ? 6 : 3, pbase = (0 != desc.format[si]) ? 3 : 0;
-  const int pone = (0 != desc.format[si]) ? 1 : 0;
-  const int S = desc.S[si], off = desc.off[si], tb = desc.tile_begin[si], G = desc.ntiles[si];
+  const int pstride = (0 != fmt) ? 6 : 3, pbase = (0 != fmt) ? 3 : 0;
+  const int pone = (0 != fmt) ? 1 : 0;
+  const int tb = s_tb[si], G = s_nt[si];
   const int lt = tile - tb, T = kSortThreads * E;
   const int t0 = min(S, lt * T), t1 = min(S, t0 + T);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w0 = min(t1, t0 + warp * 32 * E), w1 = min(t1, w0 + 32 * E);
   unsigned key[E];
   unsigned long long val[E];
-  SortCtl* const sctl = ctl + 1 + desc.gidx[si];
+  SortCtl* const sctl = ctl + 1 + s_gidx[si];
+  const unsigned blk = s_blk[si];
+  int epoch = 0; /* grid barriers passed */
   /* optional phase timestamps (stamps != nullptr): [tile][8] */
 #define XS_STAMP(slot) \
   do { \
@@ -202,14 +239,14 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
         const unsigned c = key[r];
         lo = min(lo, c);
         hi = max(hi, c);
-        gg = gcd_acc(gg, (c > c0) ? c - c0 : c0 - c);
+        if (0 == blk) gg = gcd_acc(gg, (c > c0) ? c - c0 : c0 - c);
       }
     }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if (0 == blk) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-      gg = gcd_acc(gg, __shfl_xor_sync(0xffffffffu, gg, o));
+      for (int o = 16; o > 0; o >>= 1) gg = gcd_acc(gg, __shfl_xor_sync(0xffffffffu, gg, o));
     }
     if (0 == lane) {
       s_red[0][warp] = lo;
@@ -221,7 +258,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
       for (int w = 1; w < kSortWarps; ++w) {
         lo = min(lo, s_red[0][w]);
         hi = max(hi, s_red[1][w]);
-        gg = gcd_acc(gg, s_red[2][w]);
+        if (0 == blk) gg = gcd_acc(gg, s_red[2][w]);
       }
       if (lo != 0xFFFFFFFFu) {
         atomicMax(&sctl->ncmin, ~lo);
@@ -239,27 +276,29 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     }
     for (int i = tile * kSortThreads + (int)threadIdx.x; i < desc.nzero; i += ntiles_all * kSortThreads) desc.zero[i] = 0;
     XS_STAMP(1);
-    if (!grid_sync(ctl)) return;
+    if (!grid_sync(ctl, epoch)) return;
     XS_STAMP(2);
   }
   /* per-stack digit plan; every CTA derives the same pass count and table mode for the whole batch
      (the number of grid barriers must be uniform) */
   int passes_all = 0, rows_max = 0;
-  for (int s2 = 0; s2 < desc.nstacks; ++s2) {
-    const SortCtl* const c2 = ctl + 1 + desc.gidx[s2];
-    const unsigned g2 = *(volatile const unsigned*)&c2->gcd;
+  for (int s2 = 0; s2 < nstacks; ++s2) {
+    const SortCtl* const c2 = ctl + 1 + s_gidx[s2];
+    const unsigned g2 = (0 != s_blk[s2]) ? s_blk[s2] : *(volatile const unsigned*)&c2->gcd;
     const unsigned nb2 = (0 == g2) ? 1u : (*(volatile const unsigned*)&c2->cmax - ~*(volatile const unsigned*)&c2->ncmin) / g2 + 1u;
     int b2 = 0;
     while (b2 < 32 && (nb2 - 1u) >> b2) ++b2;
     const int p2 = (b2 + kRadixBits - 1) / kRadixBits;
     if (0 == threadIdx.x) s_radix[s2] = (0 == p2) ? 1 : 1 << ((b2 + p2 - 1) / p2);
     if (p2 > passes_all) passes_all = p2;
-    if (desc.ntiles[s2] > rows_max) rows_max = desc.ntiles[s2];
+    if (s_nt[s2] > rows_max) rows_max = s_nt[s2];
   }
-  const unsigned cmin = ~*(volatile unsigned*)&sctl->ncmin, g = *(volatile unsigned*)&sctl->gcd;
+  const unsigned cmin = ~*(volatile unsigned*)&sctl->ncmin, g = (0 != blk) ? blk : *(volatile unsigned*)&sctl->gcd;
   const unsigned cmax = *(volatile unsigned*)&sctl->cmax;
   const unsigned nb = (0 == g) ? 1u : (cmax - cmin) / g + 1u;
   const double inv_g = (0 == g) ? 0.0 : 1.0 / (double)g;
+  const unsigned gm = (1u < g) ? (unsigned)((1ull << 32) / g) : 0u;
+
   int bits = 0;
   while (bits < 32 && (nb - 1u) >> bits) ++bits;
   const int passes = (bits + kRadixBits - 1) / kRadixBits;
@@ -274,7 +313,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     }
   }
   const int rb = (0 == passes) ? 0 : (bits + passes - 1) / passes, R = 1 << rb;
-  const bool direct = (size_t)rows_max * kRadix <= 32768; /* small tables: each CTA scans its stack's rows */
+  const bool direct = rows_max <= 64; /* up to 64 tiles per stack: each CTA scans its stack's rows itself */
   for (int pass = 0; pass < passes_all; ++pass) {
     const bool active = pass < passes;
     const int shift = pass * rb;
@@ -284,7 +323,9 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     int dig[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) {
-      dig[r] = (active && w0 + lane + 32 * r < w1) ? (int)((bucket_of(key[r], cmin, inv_g) >> shift) & (R - 1)) : kRadix;
+      /* bucket id: an exact quotient (g = gcd divides c - cmin) or floor((c - cmin) / blk) */
+      const unsigned id = (0 != blk) ? div_floor(key[r] - cmin, g, gm) : bucket_of(key[r], cmin, inv_g);
+      dig[r] = (active && w0 + lane + 32 * r < w1) ? (int)((id >> shift) & (R - 1)) : kRadix;
     }
     /* (a) tile histogram, row hist[tile][0..R); per-warp counters zeroed for (c) */
     for (int d = threadIdx.x; d < R; d += blockDim.x) s_base[d] = 0;
@@ -293,13 +334,14 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) {
-      if (kRadix != dig[r]) atomicAdd(&s_base[dig[r]], 1);
+    for (int r = 0; r < E; ++r) { /* one shared-memory add per distinct digit of a warp round (hot C blocks) */
+      const unsigned pr = __match_any_sync(0xffffffffu, dig[r]);
+      if (kRadix != dig[r] && 0 == __popc(pr & ((1u << lane) - 1u))) atomicAdd(&s_base[dig[r]], __popc(pr));
     }
     __syncthreads();
     for (int d = threadIdx.x; d < R; d += blockDim.x) hist[(size_t)tile * kRadix + d] = s_base[d];
     if (0 == pass) XS_STAMP(3);
-    if (!grid_sync(ctl)) return;
+    if (!grid_sync(ctl, epoch)) return;
     if (0 == pass) XS_STAMP(4);
     /* (b) digit bases of this tile inside its stack. Data written by other CTAs in this kernel is
        read with __ldcg (from L2), never through a possibly stale L1 line. Thread i owns digits
@@ -309,33 +351,60 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     int tot[PER], pre[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) tot[j] = pre[j] = 0;
-    if (direct) {
-      if (active) {
-        for (int tt = 0; tt < G; tt += 8) {
-          int h[8][PER];
+    if (direct) { /* coalesced: thread t sums digits t, t + 256, ... over the stack's rows; the sums move
+                     through shared memory to the contiguous ownership the scan below uses */
+      int ctot[PER], cpre[PER];
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
+      for (int j = 0; j < PER; ++j) ctot[j] = cpre[j] = 0;
+      if (active) {
+        for (int tt = 0; tt < G; tt += 4) {
+          int h[4][PER];
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int j = 0; j < PER; ++j) {
-              const int d = threadIdx.x * per + j;
-              h[u][j] = (j < per && tt + u < G && d < R) ? __ldcg(hist + (size_t)(tb + tt + u) * kRadix + d) : 0;
+              const int d = j * kSortThreads + (int)threadIdx.x;
+              h[u][j] = (tt + u < G && d < R) ? __ldcg(hist + (size_t)(tb + tt + u) * kRadix + d) : 0;
             }
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
+          for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int j = 0; j < PER; ++j) {
-              tot[j] += h[u][j];
-              pre[j] += (tt + u < lt) ? h[u][j] : 0;
+              ctot[j] += h[u][j];
+              cpre[j] += (tt + u < lt) ? h[u][j] : 0;
             }
         }
+      }
+      int* const s_pre = reinterpret_cast<int*>(&s_wc[0][0]); /* the per-warp counters are zero and unused until (c) */
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        const int d = j * kSortThreads + (int)threadIdx.x;
+        if (d < R) {
+          s_base[d] = ctot[j];
+          s_pre[d] = cpre[j];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        const int d = threadIdx.x * per + j;
+        const bool ok = j < per && d < R;
+        tot[j] = ok ? s_base[d] : 0;
+        pre[j] = ok ? s_pre[d] : 0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < PER; ++j) { /* the counters are zero again for (c) */
+        const int d = j * kSortThreads + (int)threadIdx.x;
+        if (d < R) s_pre[d] = 0;
       }
     }
     else { /* owner warps: one per (stack, digit), scanning that stack's tile column in place (32
               tiles per step, all loads issued first); totals to the stack's totals row */
-      for (int q = tile * kSortWarps + warp; q < desc.nstacks * kRadix; q += ntiles_all * kSortWarps) {
+      for (int q = tile * kSortWarps + warp; q < nstacks * kRadix; q += ntiles_all * kSortWarps) {
         const int s2 = q / kRadix, d = q - s2 * kRadix;
         if (d >= s_radix[s2]) continue; /* digits the stack does not use */
-        const int tb2 = desc.tile_begin[s2], G2 = desc.ntiles[s2];
+        const int tb2 = s_tb[s2], G2 = s_nt[s2];
         constexpr int kSteps = kMaxGroupTiles / 32;
         int h[kSteps];
 #pragma unroll
@@ -358,7 +427,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
         }
         if (0 == lane) hist[(size_t)(ntiles_all + s2) * kRadix + d] = run;
       }
-      if (!grid_sync(ctl)) return;
+      if (!grid_sync(ctl, epoch)) return;
 #pragma unroll
       for (int j = 0; j < PER; ++j) {
         const int d = threadIdx.x * per + j;
@@ -409,7 +478,7 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     }
     if (0 == pass) XS_STAMP(6);
     if (pass + 1 < passes_all) {
-      if (!grid_sync(ctl)) return;
+      if (!grid_sync(ctl, epoch)) return;
       if (pass + 1 < passes) {
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -438,14 +507,6 @@ constexpr int kClusterEntries = kClusterMax * kClThreads * kClE;
    every CTA of the cluster [kClusterMax][kRadix] (int) */
 constexpr size_t kClSmem = sizeof(unsigned short) * kClWarps * kRadix + sizeof(int) * kClusterMax * kRadix;
 
-/* floor(x / d) for d >= 1 from m = floor(2^32 / d) (m = 0 for d = 1): the high product is q or
-   q - 1, one correction step fixes it. */
-__device__ __forceinline__ unsigned div_floor(unsigned x, unsigned d, unsigned m) {
-  if (1u >= d) return x;
-  unsigned q = __umulhi(x, m);
-  if ((unsigned long long)(q + 1u) * d <= x) ++q;
-  return q;
-}
 
 /* Grouping of one stack of at most kClusterEntries entries by ONE thread-block cluster: a stable LSD
    counting sort over the bucket ids of the c offsets, with the same per-digit order as
@@ -464,7 +525,7 @@ template <int E>
 __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(const int* __restrict__ stack, int S, int format,
   unsigned blk, unsigned* __restrict__ k0, unsigned long long* __restrict__ v0, unsigned* __restrict__ k1,
   unsigned long long* __restrict__ v1, unsigned* __restrict__ kout, unsigned long long* __restrict__ vout,
-  int* __restrict__ seglist, int* __restrict__ zero, int nzero, SortCtl* ctl) {
+  int* __restrict__ seglist, int* __restrict__ zero, int nzero, SortCtl* ctl, int heavy) {
   namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char s_dyn[];
   unsigned short (*const s_wc)[kRadix] = reinterpret_cast<unsigned short (*)[kRadix]>(s_dyn);
@@ -626,7 +687,21 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
       tot[j] = x;
       pre[j] = p;
     }
-    block_exscan<PER>(tot, s_wsum);
+    if (1 == passes && 0 < heavy) { /* C blocks with >= heavy entries first, then the rest; id order within each */
+      int hv[PER];
+      bool isheavy[PER];
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        isheavy[j] = tot[j] >= heavy;
+        hv[j] = isheavy[j] ? tot[j] : 0;
+        tot[j] -= hv[j];
+      }
+      const int nheavy = block_exscan<PER>(hv, s_wsum);
+      block_exscan<PER>(tot, s_wsum);
+#pragma unroll
+      for (int j = 0; j < PER; ++j) tot[j] = isheavy[j] ? hv[j] : nheavy + tot[j];
+    }
+    else block_exscan<PER>(tot, s_wsum);
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
       const int d = threadIdx.x * per + j;
@@ -715,6 +790,10 @@ int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long*
     const cudaError_t r = cudaMemsetAsync(ctl, 0, sizeof(SortCtl) * (size_t)(1 + ng), s);
     if (cudaSuccess != r) return (int)r;
   }
+  else { /* a later grouping launch of the call: its grid barriers count from zero again */
+    const cudaError_t r = cudaMemsetAsync(&ctl->bar_count, 0, sizeof(unsigned), s);
+    if (cudaSuccess != r) return (int)r;
+  }
   void* args[] = {&desc, &k0, &v0, &k1, &v1, &kout, &vout, &seglist, &hist, &ctl, &stamps};
   return (int)cudaLaunchCooperativeKernel(
     large ? (const void*)xs_stack_group_kernel<16> : (const void*)xs_stack_group_kernel<8>, dim3(grid), dim3(kSortThreads),
@@ -725,7 +804,7 @@ int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long*
    cudaErrorNotSupported, launching nothing, when the device cannot run a cluster of that size. */
 int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, SortCtl* ctl, int ncta,
-  cudaStream_t s) {
+  int heavy, cudaStream_t s) {
   static int ok[XS_MAXDEV][kClusterMax + 1]; /* per device and cluster size: 0 unknown, 1 supported, -1 not */
   auto kernel = xs_stack_group_cluster_kernel<kClE>;
   int* const okp = &ok[xs_device_slot()][ncta];
@@ -753,7 +832,7 @@ int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsi
     if (cudaSuccess != r) (void)cudaGetLastError(); /* not sticky: clear it */
   }
   if (0 > *okp) return (int)cudaErrorNotSupported;
-  return (int)cudaLaunchKernelEx(&cfg, kernel, stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero, ctl);
+  return (int)cudaLaunchKernelEx(&cfg, kernel, stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero, ctl, heavy);
 }
 
 }  // namespace
@@ -796,17 +875,17 @@ int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned lon
 
 int xs_stack_group(const int* dev_stack, int S, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, void* sort_scratch, void* stream) {
-  return xs_stack_group_ex(dev_stack, S, 0, 0u, k0, v0, k1, v1, kout, vout, seglist, nullptr, 0, sort_scratch, stream);
+  return xs_stack_group_ex(dev_stack, S, 0, 0u, k0, v0, k1, v1, kout, vout, seglist, nullptr, 0, 0, sort_scratch, stream);
 }
 
 int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
-  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, void* sort_scratch,
-  void* stream) {
+  unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, int heavy,
+  void* sort_scratch, void* stream) {
   if (0 < S && S <= kClusterEntries) { /* one cluster of up to 16 CTAs */
     int ncta = 1;
     while (ncta * kClThreads * kClE < S) ncta <<= 1;
     const int r = cluster_group_launch(dev_stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero,
-      (SortCtl*)sort_scratch, ncta, (cudaStream_t)stream);
+      (SortCtl*)sort_scratch, ncta, heavy, (cudaStream_t)stream);
     if (cudaErrorNotSupported != r) return r; /* else: the cooperative kernel below */
   }
   xs_sort_batch_t d;
@@ -819,6 +898,7 @@ int xs_stack_group_ex(const int* dev_stack, int S, int format, unsigned blk, uns
   d.S[0] = S;
   d.off[0] = 0;
   d.gidx[0] = 0;
+  d.blk[0] = blk;
   return group_launch(d, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, (cudaStream_t)stream, nullptr, 1);
 }
 
@@ -867,10 +947,12 @@ int libxstream_b200_device_error(int reset) {
   return (int)e;
 }
 
-/* Diagnostic variant: the grouping of one stack with per-CTA phase timestamps (ns, %globaltimer)
+/* Diagnostic variant: the grouping of one stack (C block size blk, 0: gcd statistics) with per-CTA
+   phase timestamps (ns, %globaltimer)
    written to stamps[tile * 8 + phase]; allocates and frees its own buffers, synchronous. Returns the
    number of tiles (CTAs), or a negative CUDA error code. */
-int xs_stack_group_profile(const int* dev_stack, int S, unsigned long long* host_stamps, int capacity, void* stream) {
+int xs_stack_group_profile(const int* dev_stack, int S, unsigned blk, unsigned long long* host_stamps, int capacity,
+  void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   xs_sort_batch_t d;
   memset(&d, 0, sizeof(d));
@@ -879,6 +961,7 @@ int xs_stack_group_profile(const int* dev_stack, int S, unsigned long long* host
   d.S[0] = S;
   d.off[0] = 0;
   d.gidx[0] = 0;
+  d.blk[0] = blk;
   xs_sort_batch_t dp = d;
   int large = 0;
   const int grid = plan_tiles(&dp, &large);

@@ -53,34 +53,39 @@ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 extern "C" {
 
-/* Candidate configurations of the plain kernel for (m, n): writes up to cap (mt, nt, kp) triples. */
+/* Candidate configurations of the plain kernels for (m, n): writes up to cap (mt, nt, kp) triples,
+   the DMMA tile classes first, then (1, 1, XS_KP_FMA) when an FMA lane grid covers the block (a k
+   whose ring does not fit shared memory is timed as not applicable). */
 int xs_tune_candidates(int m, int n, int* mt_nt_kp, int cap) {
   const int mt_max = clampi((m + 7) / 8, 1, 4), nt_max = clampi((n + 7) / 8, 1, 4);
   int count = 0;
+  auto add = [&](int mt, int nt, int kp) {
+    if (count < cap && nullptr != mt_nt_kp) {
+      mt_nt_kp[3 * count + 0] = mt;
+      mt_nt_kp[3 * count + 1] = nt;
+      mt_nt_kp[3 * count + 2] = kp;
+    }
+    ++count;
+  };
   for (int mt = 1; mt <= mt_max; ++mt) {
     for (int nt = 1; nt <= nt_max; ++nt) {
-      for (int kp = 2; kp <= 4; kp += 2) {
-        if (count < cap && nullptr != mt_nt_kp) {
-          mt_nt_kp[3 * count + 0] = mt;
-          mt_nt_kp[3 * count + 1] = nt;
-          mt_nt_kp[3 * count + 2] = kp;
-        }
-        ++count;
-      }
+      for (int kp = 2; kp <= 4; kp += 2) add(mt, nt, kp);
     }
   }
+  if (xs_smm_fma_supported(m, n, 1)) add(1, 1, XS_KP_FMA);
   return count;
 }
 
 /* Times every candidate (and, with ozaki_slices > 0 and m, n, k <= 64, the Ozaki form with that
    many slices, triangle of pairs) on synthetic data; ms_out[i] = milliseconds per call of candidate
-   i (candidates in xs_tune_candidates order, the Ozaki time last). Returns the number of times
-   written, or a negative CUDA error. Synchronous; allocates and frees its own buffers. */
+   i (candidates in xs_tune_candidates order, the Ozaki time last; -1 for a candidate that does not
+   take this shape). Returns the number of times written, or a negative CUDA error. Synchronous;
+   allocates and frees its own buffers. */
 int xs_tune(int m, int n, int k, int S, int reps, int ozaki_slices, uint32_t seed, float* ms_out, int cap, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (m < 1 || n < 1 || k < 1 || S < 1 || reps < 1 || nullptr == ms_out) return -(int)cudaErrorInvalidValue;
-  int cand[3 * 32];
-  const int nc_cand = xs_tune_candidates(m, n, cand, 32);
+  int cand[3 * 33];
+  const int nc_cand = xs_tune_candidates(m, n, cand, 33);
   const int with_oz = (ozaki_slices > 0 && m <= 64 && n <= 64 && k <= 64) ? 1 : 0;
   if (cap < nc_cand + with_oz) return -(int)cudaErrorInvalidValue;
   const int na = clampi(S / 8, 16, 8192), nb = na, nc = clampi(S / 32, 8, 2048);
@@ -88,7 +93,7 @@ int xs_tune(int m, int n, int k, int S, int reps, int ozaki_slices, uint32_t see
   size_t scratch_bytes = 0;
   for (int i = 0; i < nc_cand; ++i) {
     xs_smm_params_t p = {0, cand[3 * i], cand[3 * i + 1], cand[3 * i + 2], 0, 4, 0};
-    const size_t b = xs_smm_f64_scratch_bytes(S, m, n, k, &p);
+    const size_t b = xs_smm_f64_scratch_bytes(S, m, n, k, &p); /* 0: not runnable (an FMA candidate for this k) */
     if (b > scratch_bytes) scratch_bytes = b;
   }
   if (with_oz) {
@@ -115,6 +120,10 @@ int xs_tune(int m, int n, int k, int S, int reps, int ozaki_slices, uint32_t see
   for (int i = 0; i < nc_cand + with_oz && 0 == r; ++i) {
     const bool oz = (i == nc_cand);
     xs_smm_params_t p = {0, oz ? 1 : cand[3 * i], oz ? 1 : cand[3 * i + 1], oz ? 2 : cand[3 * i + 2], 0, 4, 0};
+    if (!oz && XS_KP_FMA == p.kp && !xs_smm_fma_supported(m, n, k)) {
+      ms_out[i] = -1.f; /* the FMA kernel does not take this shape */
+      continue;
+    }
     auto call = [&]() -> int {
       if (oz) {
         return xs_launch_smm_ozaki(stack, S, m, n, k, a, na, b, nb, c, ozaki_slices, ozaki_slices - 1, scratch, scratch_bytes, s);

@@ -64,13 +64,18 @@ def random_shapes(count: int, seed: int, lo: int = 4, hi: int = 80, exclude: set
 
 def tune_one(lib, m: int, n: int, k: int, S: int, reps: int = 2, ozaki: int = 7, seed: int = 12345) -> dict:
     """Times of every applicable configuration {c: ms} and the Ozaki time (key 'oz') when measured."""
-    cand = (ctypes.c_int * (3 * K))()
-    nc = lib.libxstream_b200_tune_candidates(m, n, cand, K)
-    ms = (ctypes.c_float * (K + 1))()
-    got = lib.libxstream_b200_tune(m, n, k, S, reps, ozaki, seed, ms, K + 1, None)
+    cand = (ctypes.c_int * (3 * (K + 1)))()
+    nc = lib.libxstream_b200_tune_candidates(m, n, cand, K + 1)
+    ms = (ctypes.c_float * (K + 2))()
+    got = lib.libxstream_b200_tune(m, n, k, S, reps, ozaki, seed, ms, K + 2, None)
     if got < nc:
         raise RuntimeError(f"tune {m}x{n}x{k} S={S} failed ({got}, last error {lib.libxstream_b200_last_error()})")
-    out = {config_index(cand[3 * i], cand[3 * i + 1], cand[3 * i + 2]): float(ms[i]) for i in range(nc)}
+    out = {}
+    for i in range(nc):  # the DMMA tile classes by index; the FMA kernel (kp = -1) under "fma"
+        if ms[i] < 0:
+            continue  # the candidate does not take this shape
+        key = "fma" if cand[3 * i + 2] < 0 else config_index(cand[3 * i], cand[3 * i + 1], cand[3 * i + 2])
+        out[key] = float(ms[i])
     if got > nc:
         out["oz"] = float(ms[nc])
     return out

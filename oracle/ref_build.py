@@ -18,7 +18,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REFERENCE = Path(os.environ.get("XS_REFERENCE_ROOT", "/root/reference"))
+# The reference tree: XS_REFERENCE_ROOT, else a checkout named "reference" beside this repository. Where
+# neither exists (the GPU box), available() is False and everything that needs the tree skips.
+REFERENCE = Path(os.environ["XS_REFERENCE_ROOT"]) if os.environ.get("XS_REFERENCE_ROOT") else HERE.parent.parent / "reference"
 MULTIPLY = REFERENCE / "samples" / "smm" / "kernels" / "multiply.cl"
 TRANSPOSE = REFERENCE / "samples" / "smm" / "kernels" / "transpose.cl"
 

@@ -107,7 +107,8 @@ def test_tuner_times_every_candidate(acc):
     A, _ = acc
     lib = A.lib()
     t = P.tune_one(lib, 20, 9, 13, 2000, reps=1, ozaki=7)
-    cand = (ctypes.c_int * (3 * P.K))()
-    nc = lib.libxstream_b200_tune_candidates(20, 9, cand, P.K)
-    assert nc == 3 * 2 * 2 and len([c for c in t if c != "oz"]) == nc
+    cand = (ctypes.c_int * (3 * (P.K + 1)))()
+    nc = lib.libxstream_b200_tune_candidates(20, 9, cand, P.K + 1)
+    assert nc == 3 * 2 * 2 + 1 and len([c for c in t if c != "oz"]) == nc  # 12 DMMA tile classes + the FMA kernel
+    assert (cand[3 * 12], cand[3 * 12 + 1], cand[3 * 12 + 2]) == (1, 1, -1) and "fma" in t
     assert all(v > 0 for v in t.values()) and "oz" in t
