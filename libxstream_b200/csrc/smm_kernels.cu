@@ -149,6 +149,7 @@ struct StackTask {
   int item_begin; /* first work item of this stack (batch) */
   int cls;        /* tile class (MT - 1) * 4 + (NT - 1) (batch) */
   int sid;        /* stack index within the call: tag of its segment-list entries */
+  int kind;       /* unified batch kernel: 0 = register kernel of tile class cls, else 1 + staged shape index */
   double alpha;   /* C += alpha * A * B (1 for the LIBSMM ABI) */
   int* arrive;    /* per (CTA group, sub-tile) arrival counters of CTA-crossing segments, zero at launch:
                      the stack kernel combines them itself; nullptr: they go to the combine kernel */
@@ -650,29 +651,25 @@ __device__ __forceinline__ void drain_stage(uint64_t* bar, uint32_t parity) {
    current window) and are broadcast with shuffles. For block shapes whose C block is one warp tile.
    Every wait is bounded: a copy that does not land in time sets the grouping error word (the
    combine then writes nothing) and a device error bit, and the warp stops once the copies it has in
-   flight have landed (again bounded). */
+   flight have landed (again bounded).
+
+   One CTA group `group` (W = blockDim.x / 32 chunks) of that kernel, so that a persistent kernel can
+   run several: rings = W rings of warp_bytes(R) bytes; bars = W x R mbarriers (count 1) initialised
+   before the first item; phase = bit q: parity of the next phase of this warp's barrier q, carried
+   from item to item; meta [W][4], s_probe[2], duty[2][6] in shared memory. Returns false (uniformly
+   over the CTA) when a copy did not land in time, with no copy left in flight. Contains CTA barriers;
+   the caller separates consecutive items by one. */
 template <int M_, int N_, int K_, int R>
-__global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8))
-  xs_smm_staged_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, unsigned* __restrict__ err,
-    unsigned* __restrict__ dev_err, long long wait_limit) {
+__device__ __forceinline__ bool staged_item(const StackTask& tk, int group, int* __restrict__ seglist, unsigned* __restrict__ err,
+  long long wait_limit, unsigned char* rings, uint64_t* bars, int* meta, unsigned& phase, int* s_probe, int (*duty)[6]) {
   using G = Staged<M_, N_, K_>;
   constexpr int MT = G::MT, NT = G::NT, REGS = G::REGS, KS = G::KS;
   constexpr unsigned FULL = 0xFFFFFFFFu;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ int s_probe[2];
-  pdl_wait();
-  pdl_trigger();
-  if (0 != *(volatile const unsigned*)err) return;
   const int W = blockDim.x >> 5;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-  const int group = blockIdx.x;
-  unsigned char* const ring = smraw + (size_t)warp * G::warp_bytes(R);
-  uint64_t* const bar = (uint64_t*)(smraw + (size_t)W * G::warp_bytes(R)) + warp * R;
-  int* const meta = (int*)(smraw + (size_t)W * G::warp_bytes(R) + (size_t)W * R * sizeof(uint64_t));
+  unsigned char* const ring = rings + (size_t)warp * G::warp_bytes(R);
+  uint64_t* const bar = bars + warp * R;
   if (0 == lane) {
-#pragma unroll
-    for (int q = 0; q < R; ++q) xs_tc::mbar_init(&bar[q], 1);
-    xs_tc::fence_barrier_init();
     meta[warp * 4 + 0] = 0;
     meta[warp * 4 + 1] = 0;
     meta[warp * 4 + 2] = 0;
@@ -757,7 +754,7 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
       const unsigned long long v = val_of(e);
       const int st = (e - p0) % R;
       const bool ok =
-        __all_sync(FULL, xs_tc::mbar_wait(&bar[st], (uint32_t)(((e - p0) / R) & 1), err, 2u, wait_limit) ? 1 : 0);
+        __all_sync(FULL, xs_tc::mbar_wait(&bar[st], (((phase >> st) & 1u) + (uint32_t)((e - p0) / R)) & 1u, err, 2u, wait_limit) ? 1 : 0);
       if (!ok) {
         bad = true;
         break;
@@ -827,7 +824,14 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
       __syncwarp();
     }
     if (bad) { /* entries e .. issued - 1 have copies in flight */
-      for (int q = e - p0; q < issued; ++q) drain_stage(&bar[q % R], (uint32_t)((q / R) & 1));
+      for (int q = e - p0; q < issued; ++q) drain_stage(&bar[q % R], (((phase >> (q % R)) & 1u) + (uint32_t)(q / R)) & 1u);
+    }
+    else { /* stage q completed ceil((n - q) / R) phases in this item */
+      const int n = p1 - p0;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        if (q < n && 0 != (((n - q + R - 1) / R) & 1)) phase ^= 1u << q;
+      }
     }
   }
   __syncwarp();
@@ -857,17 +861,41 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
       meta[warp * 4 + 2] = tail;
     }
   }
-  if (__syncthreads_or(bad ? 1 : 0)) {
-    if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
-    return;
-  }
-  __shared__ int duty[2][6];
+  if (__syncthreads_or(bad ? 1 : 0)) return false;
   cta_merge<DmmaLayout<MT, NT>>(tk, group, 0, seglist, meta, W, [&](int w, int slot) -> const double* {
-    return (const double*)(smraw + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
+    return (const double*)(rings + (size_t)w * G::warp_bytes(R)) + (size_t)slot * REGS * 32;
   }, duty, (nullptr != tk.arrive && group * W < tk.nchunks) ? s_probe : nullptr);
   if (nullptr != tk.arrive) {
     __syncthreads();
-    finish_segments<DmmaLayout<MT, NT>>(tk, 0, duty, (double*)smraw);
+    finish_segments<DmmaLayout<MT, NT>>(tk, 0, duty, (double*)rings);
+  }
+  return true;
+}
+
+/* The staged stack kernel: one CTA group per CTA (see staged_item). */
+template <int M_, int N_, int K_, int R>
+__global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8))
+  xs_smm_staged_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, unsigned* __restrict__ err,
+    unsigned* __restrict__ dev_err, long long wait_limit) {
+  using G = Staged<M_, N_, K_>;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ int s_probe[2];
+  __shared__ int duty[2][6];
+  pdl_wait();
+  pdl_trigger();
+  if (0 != *(volatile const unsigned*)err) return;
+  const int W = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* const bars = (uint64_t*)(smraw + (size_t)W * G::warp_bytes(R));
+  int* const meta = (int*)(smraw + (size_t)W * G::warp_bytes(R) + (size_t)W * R * sizeof(uint64_t));
+  if (0 == lane) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) xs_tc::mbar_init(&bars[warp * R + q], 1);
+    xs_tc::fence_barrier_init();
+  }
+  __syncwarp();
+  unsigned phase = 0u;
+  if (!staged_item<M_, N_, K_, R>(tk, blockIdx.x, seglist, err, wait_limit, smraw, bars, meta, phase, s_probe, duty)) {
+    if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
   }
 }
 
@@ -1368,17 +1396,16 @@ struct BatchTasks {
   StackTask t[kMaxBatchTasks];
 };
 
-/* Register groups of the batch: group 0 holds the tile classes with MT*NT <= 9 fragments (168
-   registers, 3 CTAs per SM), group 1 the larger ones (255 registers, 2 CTAs per SM). */
+/* Register groups of the tile classes: group 0 holds the classes with MT*NT <= 9 fragments (168
+   registers: the unified batch kernel runs them), group 1 the larger ones. */
 __host__ __device__ constexpr int batch_group(int mt, int nt) { return (mt * nt <= 9) ? 0 : 1; }
-__host__ __device__ constexpr int batch_group_min_blocks(int grp) { return (0 == grp) ? 3 : 2; }
-__host__ __device__ constexpr int batch_group_max_frags(int grp) { return (0 == grp) ? 9 : 16; }
 /* k-steps per register panel: 4 for small tiles, 2 for mid-size, 1 for the largest (whose
    accumulators alone take 48-64 registers) */
 __host__ __device__ constexpr int batch_kp(int mt, int nt) { return (mt * nt <= 4) ? 4 : ((mt * nt < 12) ? 2 : 1); }
 
-/* One tile class of the batch kernel as a separate (not inlined) function, so that each class gets
-   its own register allocation instead of sharing one with the other classes' code. */
+/* One tile class of the register kernel as a separate (not inlined) function of the unified batch
+   kernel, so that each class gets its own register allocation instead of sharing one with the other
+   classes' code. */
 template <int MT, int NT>
 __device__ __noinline__ void batch_item(const StackTask& tk, int group, int sub, int* seglist, double* smem) {
   smm_item<0, 0, 0, MT, NT, batch_kp(MT, NT)>(tk, group, sub, seglist, smem);
@@ -1388,49 +1415,6 @@ template <int GRP, int MT, int NT>
 __device__ __forceinline__ void batch_dispatch(int cls, const StackTask& tk, int group, int sub, int* seglist, double* smem) {
   if constexpr (batch_group(MT, NT) == GRP) {
     if ((MT - 1) * 4 + (NT - 1) == cls) batch_item<MT, NT>(tk, group, sub, seglist, smem);
-  }
-}
-
-/* Persistent batch kernel of one register group: one launch for all stacks of the group. The grid is
-   the number of CTAs resident on the device; each CTA takes work items (CTA group x sub-tile of one
-   stack) from the group's queue, in the order the host sorted them (heaviest items first), and runs
-   them with the tile class of their stack. */
-template <int GRP>
-__global__ void __launch_bounds__(128, batch_group_min_blocks(GRP))
-  xs_smm_batch_kernel(const __grid_constant__ BatchTasks bt, int* __restrict__ seglist, unsigned* __restrict__ queue,
-    const unsigned* __restrict__ err) {
-  extern __shared__ double smem[];
-  __shared__ int s_item;
-  pdl_wait();
-  pdl_trigger();
-  if (0 != *(volatile const unsigned*)err) return;
-  for (;;) {
-    if (0 == threadIdx.x) s_item = (int)atomicAdd(queue, 1u);
-    __syncthreads();
-    const int item = s_item;
-    __syncthreads();
-    if (item >= bt.nitems) break;
-    int ti = 0;
-    while (ti + 1 < bt.ntasks && bt.t[ti + 1].item_begin <= item) ++ti;
-    const StackTask& tk = bt.t[ti];
-    const int local = item - tk.item_begin, group = local / tk.nsub, sub = local - group * tk.nsub;
-    const int cls = tk.cls;
-    batch_dispatch<GRP, 1, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 1, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 1, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 1, 4>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 2, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 2, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 2, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 2, 4>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 3, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 3, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 3, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 3, 4>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 4, 1>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 4, 2>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 4, 3>(cls, tk, group, sub, seglist, smem);
-    batch_dispatch<GRP, 4, 4>(cls, tk, group, sub, seglist, smem);
   }
 }
 
@@ -1523,47 +1507,117 @@ __global__ void __launch_bounds__(32 * kCombineWarps)
   }
 }
 
-template <int X, int MT, int NT>
-__device__ __forceinline__ void combine_dispatch(int cls, const StackTask& tk, int W, int j0, int sub, double* red) {
-  if constexpr (MT <= X && NT <= X) {
-    if ((MT - 1) * 4 + (NT - 1) == cls) combine_one<MT, NT>(tk, W, j0, sub, red);
+/* ------------------------------------------------- unified persistent batch kernel (one launch) */
+
+/* Shapes the unified batch kernel runs with their staged item function (every shape with a staged
+   kernel; 2 CTAs per SM leave 255 registers for the largest, 16 fragments); X(index, m, n, k). */
+#define XS_UNI_STAGED(X) \
+  X(0, 4, 4, 4) X(1, 8, 8, 8) X(2, 9, 9, 9) X(3, 13, 13, 13) X(4, 16, 16, 16) X(5, 22, 22, 22) X(6, 23, 23, 23) \
+  X(7, 23, 22, 13) X(8, 22, 22, 23) X(9, 32, 9, 9) X(10, 13, 4, 16) X(11, 16, 26, 5) X(12, 26, 26, 26) \
+  X(13, 26, 23, 26) X(14, 22, 32, 32) X(15, 16, 64, 9)
+constexpr int kUniMinBlocks = 2; /* CTAs per SM */
+constexpr int kUniW = 4;       /* warps per CTA */
+constexpr int kUniR = 2;       /* bulk-copy stages per warp of the staged items */
+constexpr int kUniHeader = 128; /* shared memory before an item's area: mbarriers [W][R], merge metadata [W][4] */
+constexpr size_t cmax_sz(size_t a, size_t b) { return a > b ? a : b; }
+/* shared memory of an item: the staged shapes' rings (+ slack), the register kernel's pieces (3 x 3
+   fragments at most) */
+#define XS_UNI_AREA(i, M, N, K) (size_t)kUniW * Staged<M, N, K>::warp_bytes(kUniR) + 256,
+constexpr size_t kUniAreas[] = {XS_UNI_STAGED(XS_UNI_AREA) smm_smem_bytes<4, 4>(kUniW)};
+#undef XS_UNI_AREA
+constexpr size_t uni_area_max(int i) {
+  return (i + 1 == (int)(sizeof(kUniAreas) / sizeof(*kUniAreas))) ? kUniAreas[i] : cmax_sz(kUniAreas[i], uni_area_max(i + 1));
+}
+constexpr size_t kUniArea = uni_area_max(0);
+constexpr size_t kUniSmem = kUniHeader + kUniArea;
+
+template <int M_, int N_, int K_>
+__device__ __forceinline__ bool uni_staged(const StackTask& tk, int group, int* seglist, unsigned* err, long long wait_limit,
+  unsigned char* area, uint64_t* bars, int* meta, unsigned* phase, int* s_probe, int (*duty)[6]) {
+  unsigned ph = *phase;
+  const bool ok = staged_item<M_, N_, K_, kUniR>(tk, group, seglist, err, wait_limit, area, bars, meta, ph, s_probe, duty);
+  *phase = ph;
+  return ok;
+}
+
+/* The unified persistent batch kernel: every stack of the call in one launch. The grid is the number
+   of CTAs resident on the device; each CTA takes work items (CTA group x sub-tile of one stack) from
+   one queue in the order the host laid them out (heaviest items first) and runs each with its
+   stack's kernel: the staged item function of its shape, or the register kernel of its tile class.
+   Every stack combines its CTA-crossing segments inside the kernel (arrival counters zeroed by the
+   grouping), so nothing follows. A copy that does not land in time stops the CTA with the grouping
+   error word and a device error bit set; the other CTAs stop at their next item. */
+__global__ void __launch_bounds__(32 * kUniW, kUniMinBlocks)
+  xs_smm_uni_kernel(const __grid_constant__ BatchTasks bt, int* __restrict__ seglist, unsigned* __restrict__ queue,
+    unsigned* __restrict__ err, unsigned* __restrict__ dev_err, long long wait_limit) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ int s_item, s_probe[2], duty[2][6];
+  uint64_t* const bars = (uint64_t*)smraw;
+  int* const meta = (int*)(smraw + kUniW * kUniR * sizeof(uint64_t));
+  unsigned char* const area = smraw + kUniHeader;
+  pdl_wait();
+  pdl_trigger();
+  if (__syncthreads_or((0 != *(volatile const unsigned*)err) ? 1 : 0)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (0 == lane) {
+#pragma unroll
+    for (int q = 0; q < kUniR; ++q) xs_tc::mbar_init(&bars[warp * kUniR + q], 1);
+    xs_tc::fence_barrier_init();
+  }
+  __syncwarp();
+  unsigned phase = 0u; /* bit q: parity of the next phase of this warp's barrier q */
+  for (;;) {
+    if (0 == threadIdx.x) s_item = (0 != *(volatile const unsigned*)err) ? bt.nitems : (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= bt.nitems) break;
+    int ti = 0;
+    while (ti + 1 < bt.ntasks && bt.t[ti + 1].item_begin <= item) ++ti;
+    const StackTask& tk = bt.t[ti];
+    const int local = item - tk.item_begin, group = local / tk.nsub, sub = local - group * tk.nsub;
+    bool ok = true;
+    switch (tk.kind) {
+#define XS_UNI_CASE(i, M, N, K) \
+  case 1 + i: ok = uni_staged<M, N, K>(tk, group, seglist, err, wait_limit, area, bars, meta, &phase, s_probe, duty); break;
+      XS_UNI_STAGED(XS_UNI_CASE)
+#undef XS_UNI_CASE
+      default: {
+        double* const smem = (double*)area;
+        const int cls = tk.cls;
+        batch_dispatch<0, 1, 1>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 1, 2>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 1, 3>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 1, 4>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 2, 1>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 2, 2>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 2, 3>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 2, 4>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 3, 1>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 3, 2>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 3, 3>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 4, 1>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<0, 4, 2>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<1, 3, 4>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<1, 4, 3>(cls, tk, group, sub, seglist, smem);
+        batch_dispatch<1, 4, 4>(cls, tk, group, sub, seglist, smem);
+      }
+    }
+    if (!ok) { /* uniform over the CTA */
+      if (0 == threadIdx.x && nullptr != dev_err) atomicOr(dev_err, kErrStagedTimeout);
+      break;
+    }
+    __syncthreads(); /* the next item reuses shared memory */
   }
 }
 
-/* Combine of a batch: grid-stride over segment-list entries; each entry names its stack. */
-template <int X>
-__global__ void __launch_bounds__(32 * kCombineWarps)
-  xs_smm_combine_batch_kernel(const __grid_constant__ BatchTasks bt, int W, const int* __restrict__ seglist,
-    const unsigned* __restrict__ err) {
-  extern __shared__ double red[];
-  pdl_wait();
-  if (0 != *(volatile const unsigned*)err) return;
-  const int count = seglist[0];
-  for (int li = blockIdx.x; li < count; li += gridDim.x) {
-    const int tag = seglist[1 + li], sid = tag >> 24, j0 = tag & 0xFFFFFF;
-    int ti = 0;
-    while (ti + 1 < bt.ntasks && bt.t[ti].sid != sid) ++ti;
-    const StackTask& tk = bt.t[ti];
-    for (int sub = 0; sub < tk.nsub; ++sub) {
-      const int cls = tk.cls;
-      combine_dispatch<X, 1, 1>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 1, 2>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 1, 3>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 1, 4>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 2, 1>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 2, 2>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 2, 3>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 2, 4>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 3, 1>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 3, 2>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 3, 3>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 3, 4>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 4, 1>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 4, 2>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 4, 3>(cls, tk, W, j0, sub, red);
-      combine_dispatch<X, 4, 4>(cls, tk, W, j0, sub, red);
-    }
-  }
+/* Index of (m, n, k) in the unified kernel's staged shapes, -1 if it has none. */
+int uni_staged_index(int m, int n, int k) {
+#define XS_UNI_FIND(i, M, N, K) \
+  if (M == m && N == n && K == k) return i;
+  XS_UNI_STAGED(XS_UNI_FIND)
+#undef XS_UNI_FIND
+  return -1;
 }
 
 struct SmmPlan {
@@ -1853,233 +1907,167 @@ launch_fn_t find_launcher(int m, int n, int k, const xs_smm_params_t* prm) {
   return launch_table[prm->mt - 1][prm->nt - 1][(4 == prm->kp) ? 1 : 0];
 }
 
-/* ------------------------------------------------------------------- batch of stacks (one launch) */
-
-constexpr int kBatchW = 4; /* warps per CTA of the batch kernel */
-
-size_t batch_smem_bytes(int grp) {
-  return (size_t)kBatchW * (2 * batch_group_max_frags(grp) * 2 * 32 * sizeof(double) + 4 * sizeof(int));
-}
-
-template <int GRP>
-cudaError_t batch_prepare(int* occ) {
-  static int occ_cached[XS_MAXDEV]; /* per device, 0 until set up */
-  const int dev = xs_device_slot();
-  cudaError_t r = cudaSuccess;
-  if (0 == occ_cached[dev]) {
-    const size_t smem = batch_smem_bytes(GRP);
-    int o = 0;
-    r = (cudaError_t)xs_func_smem((const void*)xs_smm_batch_kernel<GRP>, smem);
-    if (cudaSuccess == r) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, xs_smm_batch_kernel<GRP>, 32 * kBatchW, smem);
-    if (cudaSuccess != r) return r;
-    occ_cached[dev] = (o < 1) ? -1 : o;
-  }
-  if (nullptr != occ) *occ = (occ_cached[dev] < 0) ? 0 : occ_cached[dev];
-  return r;
-}
-
-cudaError_t batch_occupancy(int grp, int* occ) { return (0 == grp) ? batch_prepare<0>(occ) : batch_prepare<1>(occ); }
-
-template <int X>
-cudaError_t combine_prepare(void) {
-  const size_t csmem = sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32;
-  return (cudaError_t)xs_func_smem((const void*)xs_smm_combine_batch_kernel<X>, csmem);
-}
-
-/* Persistent stack kernel of register group GRP over the tasks in bt (their own work queue). */
-template <int GRP>
-cudaError_t batch_smm(const BatchTasks& bt, int* seglist, unsigned* queue, const unsigned* err, double flops, double bytes,
-  cudaStream_t s) {
-  int occ = 0;
-  cudaError_t r = batch_prepare<GRP>(&occ);
-  if (cudaSuccess != r) return r;
-  const int grid = max(1, min(bt.nitems, max(1, occ) * xs_sm_count()));
-  void* prof = xs_profile_begin(s);
-  r = pdl_launch(xs_smm_batch_kernel<GRP>, grid, 32 * kBatchW, batch_smem_bytes(GRP), s, bt, seglist, queue, err);
-  xs_profile_end(prof, "smm_batch", flops, bytes, s);
-  return r;
-}
-
-/* Combine of all CTA-crossing segments of the batch (bt: every task of the call). */
-template <int X>
-cudaError_t batch_combine(const BatchTasks& bt, int ngroups_total, int* seglist, const unsigned* err, cudaStream_t s) {
-  cudaError_t r = combine_prepare<X>();
-  if (cudaSuccess != r) return r;
-  void* prof = xs_profile_begin(s);
-  const int cgrid = max(1, min(ngroups_total, 2 * xs_sm_count()));
-  r = pdl_launch(xs_smm_combine_batch_kernel<X>, cgrid, 32 * kCombineWarps, sizeof(double) * (kCombineWarps - 1) * (X * X * 2) * 32,
-    s, bt, kBatchW, seglist, err);
-  xs_profile_end(prof, "combine_batch", 0.0, 0.0, s);
-  return r;
-}
+/* ------------------------------------------------------------- unified batch: plan and launch */
 
 /* One part of a batch: a stack, or a slice of a stack larger than one grouping launch takes. */
-struct BatchPart {
-  int stack; /* index into the caller's array */
-  int first; /* first entry of the slice */
-  int S;
-  int mt, nt;
-  int solo; /* large enough to fill the device alone: runs as its own (shape-specialised) launch */
+struct UniPart {
+  int stack, first, S;
+  int kind;   /* 0: register kernel of tile class (mt, nt); else 1 + staged shape index */
+  int mt, nt; /* warp tile in 8 x 8 fragments */
+  int nsub, nsub_n, L, ngroups;
   double item_cost;
-  xs_smm_params_t prm;
 };
 
-/* A part whose one-wave chunk length (as a launch of its own) reaches this many entries keeps the
-   device busy by itself; it runs with the single-stack kernel of its shape instead of the queue. */
-constexpr int kSoloMinL = 16;
+/* Work items per resident CTA the plan aims for: enough for the queue to even out items of unequal
+   speed, few enough that an item's start (first copies in flight) and merge stay a small share. A
+   batch of one part has items of equal speed: one per CTA. Otherwise one per kUniItemCost cost units
+   of work per CTA, between 6 and 16 (measured on B200: a 186k-triple mixed batch, 25k units per CTA,
+   is fastest with 6 items per CTA, a 2M-triple one, 275k units, with 12-24). */
+constexpr double kUniItemsMin = 6.0, kUniItemsMax = 16.0, kUniItemCost = 4000.0;
 
-struct BatchPlan {
-  int nparts, X, ntotal, ngroups_total, nitems;
-  BatchPart part[kMaxBatchTasks];
-  int L[kMaxBatchTasks], nsub[kMaxBatchTasks], nsub_n[kMaxBatchTasks], ngroups[kMaxBatchTasks];
-  size_t off_part[kMaxBatchTasks], pieces_off[kMaxBatchTasks];
+struct UniPlan {
+  int nparts, ntotal, nitems, ngroups_total, occ;
+  UniPart part[kMaxBatchTasks];
   int order[kMaxBatchTasks]; /* parts by descending item cost */
-  size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces, off_sort;
-  size_t off_arrive, narrive;             /* arrival counters of the solo parts (in-kernel combine) */
-  size_t arrive_off[kMaxBatchTasks];
-  size_t total;
+  size_t off_part[kMaxBatchTasks], pieces_off[kMaxBatchTasks], arrive_off[kMaxBatchTasks];
+  size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces;
+  size_t off_arrive, narrive, off_sort, total;
 };
 
-/* Work decomposition of a batch: stacks split into parts of at most xs_stack_group_max() entries;
-   per part a tile class (MT x NT from the parameter table) and a chunk length L chosen so that every
-   work item (W chunks x one sub-tile) costs about the same, ~4 items per resident CTA. */
-int plan_batch(const libxstream_b200_stack_t* st, int ns, BatchPlan* bp) {
+/* Tile of at most 4 x 4 fragments for a block of fm x fn fragments: the fewest padded fragments,
+   then the fewest sub-tiles. */
+void uni_tiles(int fm, int fn, int* mt, int* nt) {
+  long best = -1;
+  for (int a = 1; a <= 4; ++a) {
+    for (int b = 1; b <= 4; ++b) {
+      const long subs = (long)((fm + a - 1) / a) * ((fn + b - 1) / b);
+      const long cost = subs * a * b * 64 + subs;
+      if (best < 0 || cost < best) {
+        best = cost;
+        *mt = a;
+        *nt = b;
+      }
+    }
+  }
+}
+
+/* CTAs of the unified kernel resident per SM on the active device (cached per device). */
+int uni_occupancy(void) {
+  static int occ_cached[XS_MAXDEV]; /* 0 until set up */
+  const int dev = xs_device_slot();
+  if (0 == occ_cached[dev]) {
+    int o = 0;
+    if (cudaSuccess != (cudaError_t)xs_func_smem((const void*)xs_smm_uni_kernel, kUniSmem) ||
+        cudaSuccess != cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, xs_smm_uni_kernel, 32 * kUniW, kUniSmem) || o < 1) {
+      return 0;
+    }
+    occ_cached[dev] = o;
+  }
+  return occ_cached[dev];
+}
+
+/* Work decomposition of a batch for the unified kernel: stacks split into parts of at most
+   xs_stack_group_max() entries; per part its kernel (the staged item function of its shape, or the
+   register kernel of a tile class of at most 4 x 4 fragments) and a chunk length L chosen so that every
+   work item (kUniW chunks x one sub-tile) costs about the same (kUniItemsMin..kUniItemsMax items per
+   resident CTA). Returns the
+   number of parts, -1 if the batch has too many parts or the kernel cannot be set up. */
+int plan_uni(const libxstream_b200_stack_t* st, int ns, UniPlan* up) {
   const int smax = xs_stack_group_max();
-  bp->nparts = 0;
-  bp->X = 1;
-  bp->ntotal = 0;
+  up->nparts = 0;
+  up->ntotal = 0;
   for (int i = 0; i < ns; ++i) {
     if (0 >= st[i].stack_size) continue;
+    const int m = st[i].m, n = st[i].n, k = st[i].k, fm = (m + 7) / 8, fn = (n + 7) / 8;
     xs_smm_params_t prm;
-    xs_params_lookup(3, st[i].m, st[i].n, st[i].k, st[i].stack_size, &prm);
-    if (4 < prm.wpb) prm.wpb = kBatchW; /* batch parts run kBatchW chunks per CTA */
+    xs_params_lookup(3, m, n, k, st[i].stack_size, &prm);
+    const int sidx = uni_staged_index(m, n, k);
+    int mt = prm.mt, nt = prm.nt;
+    if (0 > sidx && (mt > fm || nt > fn)) uni_tiles(fm, fn, &mt, &nt);
     for (int first = 0; first < st[i].stack_size; first += smax) {
-      if (bp->nparts == kMaxBatchTasks) return -1;
-      BatchPart& p = bp->part[bp->nparts++];
+      if (up->nparts == kMaxBatchTasks) return -1;
+      UniPart& p = up->part[up->nparts++];
       p.stack = i;
       p.first = first;
       p.S = min(smax, st[i].stack_size - first);
-      p.mt = prm.mt;
-      p.nt = prm.nt;
-      p.prm = prm;
-      p.solo = 0;
-      if (p.mt > bp->X) bp->X = p.mt;
-      if (p.nt > bp->X) bp->X = p.nt;
-      bp->ntotal += p.S;
+      p.kind = (0 <= sidx) ? 1 + sidx : 0;
+      p.mt = (0 <= sidx) ? fm : mt;
+      p.nt = (0 <= sidx) ? fn : nt;
+      p.nsub_n = (0 <= sidx) ? 1 : (fn + p.nt - 1) / p.nt;
+      p.nsub = (0 <= sidx) ? 1 : ((fm + p.mt - 1) / p.mt) * p.nsub_n;
+      up->ntotal += p.S;
     }
   }
-  if (0 == bp->nparts) return 0;
-  /* large parts run alone, one wave of the single-stack kernel each; the rest share the queue.
-     Cost units: DMMA instructions per entry per warp plus a fixed per-entry overhead; each register
-     group gets items of equal cost, about two per CTA resident in that group's launch */
-  double total[2] = {0, 0};
-  int solo_L[kMaxBatchTasks];
-  for (int q = 0; q < bp->nparts; ++q) {
-    BatchPart& p = bp->part[q];
-    const libxstream_b200_stack_t& d = st[p.stack];
-    const int nsub = (XS_KP_FMA == p.prm.kp) ? 1 : ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
-    SmmPlan pl = {};
-    pl.W = kBatchW;
-    StackTask none = {};
-    none.m = d.m;
-    none.n = d.n;
-    none.k = d.k;
-    int occ = 0;
-    if (cudaSuccess != find_launcher(d.m, d.n, d.k, &p.prm)(pl, none, nullptr, nullptr, 0, &occ) || occ < 1) occ = 1;
-    const long resident = (long)occ * xs_sm_count();
-    solo_L[q] = (int)(((long)p.S * nsub + resident * kBatchW - 1) / (resident * kBatchW));
-    p.solo = (solo_L[q] >= kSoloMinL) ? 1 : 0;
-    if (!p.solo && XS_KP_FMA == p.prm.kp) { /* the persistent kernels run DMMA tiles only */
-      xs_params_default(d.m, d.n, d.k, p.S, &p.prm);
-      if (0 == p.prm.kp) p.prm.kp = 2;
-      p.mt = p.prm.mt;
-      p.nt = p.prm.nt;
-    }
-    if (!p.solo && (p.mt > 4 || p.nt > 4)) { /* the persistent kernels take tiles of up to 4 x 4 fragments */
-      p.mt = p.prm.mt = min(p.mt, 4);
-      p.nt = p.prm.nt = min(p.nt, 4);
-      if (0 == p.prm.kp) p.prm.kp = 2;
-    }
-    if (!p.solo) {
-      const int nsub2 = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * ((((d.n + 7) / 8) + p.nt - 1) / p.nt);
-      total[batch_group(p.mt, p.nt)] += (double)p.S * nsub2 * (p.mt * p.nt * ((d.k + 3) / 4) + 8);
-    }
+  if (0 == up->nparts) return 0;
+  up->occ = uni_occupancy();
+  if (0 >= up->occ) return -1;
+  /* cost units: DMMA instructions per entry per warp plus a fixed per-entry overhead */
+  double total = 0;
+  for (int q = 0; q < up->nparts; ++q) {
+    const UniPart& p = up->part[q];
+    total += (double)p.S * p.nsub * (p.mt * p.nt * ((st[p.stack].k + 3) / 4) + 8);
   }
-  bp->X = 1; /* the batch combine serves the shared-queue parts only: solo parts combine in their kernel */
-  for (int q = 0; q < bp->nparts; ++q) {
-    if (bp->part[q].solo) continue;
-    bp->X = max(bp->X, max(bp->part[q].mt, bp->part[q].nt));
-  }
-  double target[2];
-  for (int grp = 0; grp < 2; ++grp) {
-    int occ = 0;
-    if (cudaSuccess != batch_occupancy(grp, &occ) || occ < 1) occ = 1;
-    target[grp] = total[grp] / ((double)occ * xs_sm_count() * 2.0);
-  }
+  const double per_cta = total / ((double)up->occ * xs_sm_count());
+  const double items = (1 == up->nparts) ? 1.0 : fmin(kUniItemsMax, fmax(kUniItemsMin, per_cta / kUniItemCost));
+  const double target = per_cta / items;
   size_t off = 0, poff = 0, narrive = 0;
-  bp->ngroups_total = 0;
-  bp->nitems = 0;
-  for (int q = 0; q < bp->nparts; ++q) {
-    BatchPart& p = bp->part[q];
-    const libxstream_b200_stack_t& d = st[p.stack];
-    bp->nsub_n[q] = (((d.n + 7) / 8) + p.nt - 1) / p.nt;
-    bp->nsub[q] = ((((d.m + 7) / 8) + p.mt - 1) / p.mt) * bp->nsub_n[q];
-    if (XS_KP_FMA == p.prm.kp) bp->nsub_n[q] = bp->nsub[q] = 1; /* the FMA lane grid covers the block */
-    const double per_entry = p.mt * p.nt * ((d.k + 3) / 4) + 8;
-    long L = p.solo ? solo_L[q] : (long)(target[batch_group(p.mt, p.nt)] / (kBatchW * per_entry) + 0.5);
+  up->ngroups_total = 0;
+  up->nitems = 0;
+  for (int q = 0; q < up->nparts; ++q) {
+    UniPart& p = up->part[q];
+    const double per_entry = p.mt * p.nt * ((st[p.stack].k + 3) / 4) + 8;
+    long L = (long)(target / (kUniW * per_entry) + 0.5);
     if (L < 1) L = 1;
     if (L > p.S) L = p.S;
-    bp->L[q] = (int)L;
+    p.L = (int)L;
     const int nchunks = (int)((p.S + L - 1) / L);
-    bp->ngroups[q] = (nchunks + kBatchW - 1) / kBatchW;
-    p.item_cost = (double)kBatchW * L * per_entry;
-    bp->off_part[q] = off;
+    p.ngroups = (nchunks + kUniW - 1) / kUniW;
+    p.item_cost = (double)kUniW * L * per_entry;
+    up->off_part[q] = off;
     off += (size_t)p.S;
-    bp->pieces_off[q] = poff;
-    const int regs = (XS_KP_FMA == p.prm.kp) ? fma_piece_regs(d.m, d.n, d.k) : p.mt * p.nt * 2;
-    if (0 >= regs) return -1;
-    poff += (size_t)2 * bp->ngroups[q] * bp->nsub[q] * regs * 32;
-    bp->arrive_off[q] = narrive;
-    if (p.solo) narrive += (size_t)3 * bp->ngroups[q] * bp->nsub[q];
-    bp->ngroups_total += bp->ngroups[q];
-    if (!p.solo) bp->nitems += bp->ngroups[q] * bp->nsub[q];
-    bp->order[q] = q;
+    up->pieces_off[q] = poff;
+    poff += (size_t)2 * p.ngroups * p.nsub * (p.mt * p.nt * 2) * 32;
+    up->arrive_off[q] = narrive;
+    narrive += (size_t)3 * p.ngroups * p.nsub;
+    up->ngroups_total += p.ngroups;
+    up->nitems += p.ngroups * p.nsub;
+    up->order[q] = q;
   }
-  for (int a = 1; a < bp->nparts; ++a) { /* heaviest items first (insertion sort, stable) */
-    const int v = bp->order[a];
+  for (int a = 1; a < up->nparts; ++a) { /* heaviest items first (insertion sort, stable) */
+    const int v = up->order[a];
     int b = a - 1;
-    while (b >= 0 && bp->part[bp->order[b]].item_cost < bp->part[v].item_cost) {
-      bp->order[b + 1] = bp->order[b];
+    while (b >= 0 && up->part[up->order[b]].item_cost < up->part[v].item_cost) {
+      up->order[b + 1] = up->order[b];
       --b;
     }
-    bp->order[b + 1] = v;
+    up->order[b + 1] = v;
   }
-  const size_t N = (size_t)bp->ntotal;
+  const size_t N = (size_t)up->ntotal;
   size_t o = 0;
   const size_t ks = align_up(sizeof(unsigned) * N, 256), vs = align_up(sizeof(unsigned long long) * N, 256);
-  bp->off_keys_in = o;
+  up->off_keys_in = o;
   o += ks;
-  bp->off_keys_tmp = o;
+  up->off_keys_tmp = o;
   o += ks;
-  bp->off_keys_out = o;
+  up->off_keys_out = o;
   o += ks;
-  bp->off_vals_in = o;
+  up->off_vals_in = o;
   o += vs;
-  bp->off_vals_tmp = o;
+  up->off_vals_tmp = o;
   o += vs;
-  bp->off_vals_out = o;
+  up->off_vals_out = o;
   o += vs;
-  bp->off_seglist = o;
-  o = align_up(o + sizeof(int) * ((size_t)bp->ngroups_total + 1), 256);
-  bp->off_pieces = o;
+  up->off_seglist = o;
+  o = align_up(o + sizeof(int) * ((size_t)up->ngroups_total + 1), 256);
+  up->off_pieces = o;
   o = align_up(o + sizeof(double) * poff, 256);
-  bp->off_arrive = o;
-  bp->narrive = narrive;
+  up->off_arrive = o;
+  up->narrive = narrive;
   o = align_up(o + sizeof(int) * narrive, 256);
-  bp->off_sort = o;
+  up->off_sort = o;
   o = align_up(o + xs_sort_ctl_bytes() + sizeof(int) * ((size_t)xs_sort_launch_tiles() + XS_MAX_BATCH) * 2048, 256);
-  bp->total = o;
-  return bp->nparts;
+  up->total = o;
+  return up->nparts;
 }
 
 /* ------------------------------------------------------------------------------ transpose */
@@ -2296,43 +2284,46 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
 }
 
 size_t xs_smm_batch_scratch_bytes(const libxstream_b200_stack_t* stacks, int nstacks) {
-  BatchPlan bp;
-  if (0 >= plan_batch(stacks, nstacks, &bp)) return 0;
-  return bp.total;
+  UniPlan up;
+  if (0 >= plan_uni(stacks, nstacks, &up)) return 0;
+  return up.total;
 }
 
+/* A batch of stacks: one grouping launch for up to XS_MAX_BATCH parts (more only when the parts
+   exceed the tiles one grouping launch takes), then one launch of the unified persistent kernel for
+   every part; no combine launch. */
 int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch, size_t scratch_bytes, void* stream) {
-  BatchPlan bp;
+  UniPlan up;
   cudaStream_t s = (cudaStream_t)stream;
-  const int np = plan_batch(st, ns, &bp);
+  const int np = plan_uni(st, ns, &up);
   if (0 > np) return (int)cudaErrorInvalidValue;
   if (0 == np) return 0;
-  if (scratch_bytes < bp.total || nullptr == scratch) return (int)cudaErrorInvalidValue;
+  if (scratch_bytes < up.total || nullptr == scratch) return (int)cudaErrorInvalidValue;
   char* const base = (char*)scratch;
-  unsigned* const k0 = (unsigned*)(base + bp.off_keys_in);
-  unsigned* const k1 = (unsigned*)(base + bp.off_keys_tmp);
-  unsigned* const kout = (unsigned*)(base + bp.off_keys_out);
-  unsigned long long* const v0 = (unsigned long long*)(base + bp.off_vals_in);
-  unsigned long long* const v1 = (unsigned long long*)(base + bp.off_vals_tmp);
-  unsigned long long* const vout = (unsigned long long*)(base + bp.off_vals_out);
-  int* const seglist = (int*)(base + bp.off_seglist);
-  double* const pieces = (double*)(base + bp.off_pieces);
-  void* const sort_scratch = base + bp.off_sort;
-  int* const arrive = (int*)(base + bp.off_arrive);
+  unsigned* const k0 = (unsigned*)(base + up.off_keys_in);
+  unsigned* const k1 = (unsigned*)(base + up.off_keys_tmp);
+  unsigned* const kout = (unsigned*)(base + up.off_keys_out);
+  unsigned long long* const v0 = (unsigned long long*)(base + up.off_vals_in);
+  unsigned long long* const v1 = (unsigned long long*)(base + up.off_vals_tmp);
+  unsigned long long* const vout = (unsigned long long*)(base + up.off_vals_out);
+  int* const seglist = (int*)(base + up.off_seglist);
+  double* const pieces = (double*)(base + up.off_pieces);
+  void* const sort_scratch = base + up.off_sort;
+  int* const arrive = (int*)(base + up.off_arrive);
   /* grouping: one control block for the call, then as few grouping launches as the tiles need; the
-     first one also zeroes the solo parts' arrival counters */
-  int r = xs_sort_clear_ctl(sort_scratch, bp.nparts, s);
+     first one also zeroes every part's arrival counters */
+  int r = xs_sort_clear_ctl(sort_scratch, up.nparts, s);
   if (0 != r) return r;
   void* prof = xs_profile_begin(s);
   xs_sort_batch_t sb;
   memset(&sb, 0, sizeof(sb));
-  sb.zero = (0 < bp.narrive) ? arrive : nullptr;
-  sb.nzero = (int)bp.narrive;
+  sb.zero = (0 < up.narrive) ? arrive : nullptr;
+  sb.nzero = (int)up.narrive;
   int tiles = 0;
   const int launch_tiles = xs_sort_launch_tiles(), tile_entries = xs_sort_tile_entries(1);
-  for (int q = 0; q <= bp.nparts; ++q) {
-    const int nt = (q < bp.nparts) ? (bp.part[q].S + tile_entries - 1) / tile_entries : 0;
-    if (q == bp.nparts || sb.nstacks == XS_MAX_BATCH || tiles + nt > launch_tiles) {
+  for (int q = 0; q <= up.nparts; ++q) {
+    const int nt = (q < up.nparts) ? (up.part[q].S + tile_entries - 1) / tile_entries : 0;
+    if (q == up.nparts || sb.nstacks == XS_MAX_BATCH || tiles + nt > launch_tiles) {
       if (0 < sb.nstacks) {
         r = xs_stack_group_batch(&sb, k0, v0, k1, v1, kout, vout, seglist, sort_scratch, s);
         if (0 != r) return r;
@@ -2342,87 +2333,59 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
       sb.nstacks = 0;
       tiles = 0;
     }
-    if (q == bp.nparts) break;
-    const BatchPart& p = bp.part[q];
+    if (q == up.nparts) break;
+    const UniPart& p = up.part[q];
     sb.gidx[sb.nstacks] = q;
     sb.stack[sb.nstacks] = st[p.stack].dev_param_stack + 3 * (size_t)p.first;
     sb.format[sb.nstacks] = 0;
     sb.S[sb.nstacks] = p.S;
-    sb.off[sb.nstacks] = (int)bp.off_part[q];
+    sb.off[sb.nstacks] = (int)up.off_part[q];
     sb.blk[sb.nstacks] = (unsigned)(st[p.stack].m * st[p.stack].n);
     ++sb.nstacks;
     tiles += nt;
   }
-  xs_profile_end(prof, "sort", 0.0, 48.0 * bp.ntotal, s);
-  /* task table of the whole call (for the combine); one launch of the single-stack kernel per solo
-     part and one persistent launch per register group for the others: every group runs at the
-     occupancy its largest tiles allow */
-  BatchTasks all, grp[2];
-  memset(&all, 0, sizeof(all));
-  memset(grp, 0, sizeof(grp));
-  double gflops[2] = {0, 0}, gbytes[2] = {0, 0};
-  for (int i = 0; i < bp.nparts; ++i) {
-    const int q = bp.order[i];
-    const BatchPart& p = bp.part[q];
+  xs_profile_end(prof, "sort", 0.0, 48.0 * up.ntotal, s);
+  /* task table in item order (heaviest items first) */
+  BatchTasks bt;
+  memset(&bt, 0, sizeof(bt));
+  double flops = 0, bytes = 0;
+  for (int i = 0; i < up.nparts; ++i) {
+    const int q = up.order[i];
+    const UniPart& p = up.part[q];
     const libxstream_b200_stack_t& d = st[p.stack];
     StackTask tk = {};
     tk.alpha = 1.0;
     tk.a = (const double*)d.a;
     tk.b = (const double*)d.b;
     tk.c = (double*)d.c;
-    tk.keys = kout + bp.off_part[q];
-    tk.vals = vout + bp.off_part[q];
-    tk.pieces = pieces + bp.pieces_off[q];
+    tk.keys = kout + up.off_part[q];
+    tk.vals = vout + up.off_part[q];
+    tk.pieces = pieces + up.pieces_off[q];
+    tk.arrive = arrive + up.arrive_off[q];
     tk.S = p.S;
     tk.m = d.m;
     tk.n = d.n;
     tk.k = d.k;
-    tk.L = bp.L[q];
-    tk.nchunks = (p.S + bp.L[q] - 1) / bp.L[q];
-    tk.ngroups = bp.ngroups[q];
-    tk.nsub_n = bp.nsub_n[q];
-    tk.nsub = bp.nsub[q];
+    tk.L = p.L;
+    tk.nchunks = (p.S + p.L - 1) / p.L;
+    tk.ngroups = p.ngroups;
+    tk.nsub_n = p.nsub_n;
+    tk.nsub = p.nsub;
     tk.cls = (p.mt - 1) * 4 + (p.nt - 1);
+    tk.kind = p.kind;
     tk.sid = q;
-    tk.item_begin = all.nitems;
-    all.t[all.ntasks++] = tk;
-    all.nitems += tk.ngroups * tk.nsub;
-    if (p.solo) {
-      SmmPlan pl = {};
-      pl.W = kBatchW;
-      pl.L = tk.L;
-      pl.nchunks = tk.nchunks;
-      pl.ngroups = tk.ngroups;
-      pl.nsub_n = tk.nsub_n;
-      pl.nsub = tk.nsub;
-      pl.no_combine = 1;
-      tk.arrive = arrive + bp.arrive_off[q]; /* its CTA-crossing segments are combined in its kernel */
-      r = (int)find_launcher(d.m, d.n, d.k, &p.prm)(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
-      if (0 != r) return r;
-      continue;
-    }
-    const int X = batch_group(p.mt, p.nt);
-    BatchTasks& b = grp[X];
-    tk.item_begin = b.nitems;
-    b.t[b.ntasks++] = tk;
-    b.nitems += tk.ngroups * tk.nsub;
-    gflops[X] += 2.0 * d.m * d.n * d.k * (double)p.S;
-    gbytes[X] += 8.0 * p.S * ((double)d.m * d.k + (double)d.k * d.n + 2.0 * d.m * d.n);
+    tk.item_begin = bt.nitems;
+    bt.t[bt.ntasks++] = tk;
+    bt.nitems += p.ngroups * p.nsub;
+    flops += 2.0 * d.m * d.n * d.k * (double)p.S;
+    bytes += 8.0 * p.S * ((double)d.m * d.k + (double)d.k * d.n + 2.0 * d.m * d.n);
   }
-  const unsigned* const err = xs_sort_error_flag(sort_scratch);
-  for (int X = 0; X < 2 && 0 == r; ++X) {
-    if (0 == grp[X].ntasks) continue;
-    unsigned* const queue = xs_sort_queue_counter(sort_scratch, X);
-    r = (0 == X) ? (int)batch_smm<0>(grp[X], seglist, queue, err, gflops[X], gbytes[X], s)
-                 : (int)batch_smm<1>(grp[X], seglist, queue, err, gflops[X], gbytes[X], s);
-  }
-  if (0 != r) return r;
-  switch (bp.X) {
-    case 1: return (int)batch_combine<1>(all, bp.ngroups_total, seglist, err, s);
-    case 2: return (int)batch_combine<2>(all, bp.ngroups_total, seglist, err, s);
-    case 3: return (int)batch_combine<3>(all, bp.ngroups_total, seglist, err, s);
-    default: return (int)batch_combine<4>(all, bp.ngroups_total, seglist, err, s);
-  }
+  const int grid = max(1, min(bt.nitems, up.occ * xs_sm_count()));
+  prof = xs_profile_begin(s);
+  r = (int)pdl_launch(xs_smm_uni_kernel, grid, 32 * kUniW, kUniSmem, s, bt, seglist, xs_sort_queue_counter(sort_scratch, 0),
+    (unsigned*)xs_sort_error_flag(sort_scratch), xs_device_error_ptr(), xs_wait_limit());
+  xs_profile_end(prof, "smm_batch", flops, bytes, s);
+  return r;
 }
 
 int xs_launch_transpose(const int* trs, int offset, int S, void* data, int esize, int m, int n, void* stream) {

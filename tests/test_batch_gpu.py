@@ -1,6 +1,7 @@
 """GPU parity tests of the batched stack path (libxstream_b200_process_batch): all stacks of one
-multiplication in one call -- one grouping pass, one persistent stack kernel, one combine -- against
-the CPU oracle (relative max-norm error per C block <= 1e-13), with CUDA-graph capture/replay."""
+multiplication in one call -- one grouping pass, then one persistent kernel that runs every stack's
+work items and combines their CTA-crossing segments itself -- against the CPU oracle (relative
+max-norm error per C block <= 1e-13), with CUDA-graph capture/replay."""
 from __future__ import annotations
 
 import ctypes
@@ -92,7 +93,7 @@ def test_batch_deterministic_and_graph_replay(acc):
     assert lib.libxstream_b200_graph_begin(stream.handle) == 0
     rc = run_batch(A, stream, devs)
     assert lib.libxstream_b200_graph_end(stream.handle, ctypes.byref(gexec), ctypes.byref(nk)) == 0
-    assert rc == 0 and nk.value >= 3  # grouping + persistent stack kernel + combine
+    assert rc == 0 and nk.value == 2  # one grouping launch + the persistent kernel: no combine launch
     for _ in range(2):
         assert lib.libxstream_b200_graph_launch(gexec, stream.handle) == 0
     stream.sync()
@@ -162,10 +163,11 @@ def test_batch_rejects_unsuitable_stacks(acc):
     d.free()
 
 
-def test_batch_solo_parts_combine_in_kernel(acc):
-    """Large parts run alone and combine their CTA-crossing segments inside their own kernel (staged
-    kernels, one with a 2 x 8-fragment tile); small parts of the same shapes share the persistent
-    kernels (tiles clamped to 4 x 4) and the batch combine. Parity and bitwise reproducibility."""
+def test_batch_mixed_item_kinds(acc):
+    """Large and small stacks of the same shapes in one persistent launch: 23^3 and 16x64x9 items run
+    their staged item functions (16x64x9 with a 2 x 8-fragment tile), 45^3 items the register kernel
+    with sub-tiles; every stack combines its CTA-crossing segments in the kernel. Parity and bitwise
+    reproducibility."""
     A, stream = acc
     cases = [W.stack_case(16, 64, 9, 120000, 2000, 2000, 500, seed=701),
              W.stack_case(16, 64, 9, 900, 100, 100, 30, seed=702),
