@@ -1,12 +1,13 @@
 /*
  * Learned parameter predictor: a 3-layer MLP (FP32, width 64) that maps a stack's shape
  * (m, n, k, stack size, exponent spread of the inputs) to the autotuner's best kernel configuration
- * (one of 32 tile classes MT x NT x KP) and to the plain-vs-Ozaki choice. The counterpart of the
+ * (one of 32 DMMA tile classes MT x NT x KP, or the register-blocked FMA kernel) and to the
+ * plain-vs-Ozaki choice. The counterpart of the
  * reference's learned parameter prediction (samples/smm/tune_multiply.py driving LIBXS predict
  * models, params/*.bin), rebuilt as this library's own network and kernels.
  *
  * Network: x (27 features) -> h1 = relu(x W1 + b1) (64) -> h2 = relu(h1 W2 + b2) (64) -> y = h2 W3 + b3
- * (33 outputs: 32 configuration logits, 1 Ozaki logit). Features: one-hot ceil(m/8) and ceil(n/8)
+ * (34 outputs: 32 DMMA configuration logits, the FMA kernel's logit, 1 Ozaki logit). Features: one-hot ceil(m/8) and ceil(n/8)
  * (the 8x8 DMMA fragment counts, 1..10, which decide the tile classes), log2 k / 6.5, (k mod 8)/8,
  * log10 S / 5, spread / 40, log2(m n k S) / 40, (m mod 8)/8, (n mod 8)/8.
  * Loss per sample: cross-entropy of the masked softmax p against the soft target
@@ -28,7 +29,7 @@
 
 #define XS_MLP_F 27
 #define XS_MLP_H 64
-#define XS_MLP_K 32
+#define XS_MLP_K 33 /* configurations: 32 DMMA tile classes, then the FMA kernel (index 32) */
 #define XS_MLP_O (XS_MLP_K + 1)
 #define XS_MLP_NW (XS_MLP_F * XS_MLP_H + XS_MLP_H + XS_MLP_H * XS_MLP_H + XS_MLP_H + XS_MLP_H * XS_MLP_O + XS_MLP_O)
 
@@ -40,8 +41,12 @@ constexpr int kWChunks = 16; /* sample chunks of the weight-gradient reduction *
 
 __host__ __device__ inline int mt_max_of(int m) { return min(4, max(1, (m + 7) / 8)); }
 
-/* configuration c = (mt-1)*8 + (nt-1)*2 + (kp == 4) applies to (m, n) */
-__host__ __device__ inline bool config_valid(int c, int m, int n) { return (c >> 3) + 1 <= mt_max_of(m) && ((c >> 1) & 3) + 1 <= mt_max_of(n); }
+/* configuration c = (mt-1)*8 + (nt-1)*2 + (kp == 4) applies to (m, n); c = 32, the FMA kernel, where the
+   caller says it does (fma_ok: its lane grids cover the block and its ring fits shared memory) */
+constexpr int kFmaConfig = 32;
+__host__ __device__ inline bool config_valid(int c, int m, int n, bool fma_ok) {
+  return (kFmaConfig == c) ? fma_ok : ((c >> 3) + 1 <= mt_max_of(m) && ((c >> 1) & 3) + 1 <= mt_max_of(n));
+}
 
 __device__ void features(const int* raw, float* x) {
   const float k = (float)raw[2], S = fmaxf((float)raw[3], 1.f);
@@ -216,23 +221,24 @@ __global__ void xs_mlp_adam(float* __restrict__ W, const float* __restrict__ G, 
 
 /* Inference, after xs_mlp_fwd: masked argmax over the configurations, its softmax probability and
    the Ozaki probability. */
-__global__ void xs_mlp_select(const float* __restrict__ Y, const int* __restrict__ raw, int N, unsigned char* __restrict__ cfg,
-  float* __restrict__ conf, float* __restrict__ pz) {
+__global__ void xs_mlp_select(const float* __restrict__ Y, const int* __restrict__ raw, const unsigned char* __restrict__ fma_ok,
+  int N, unsigned char* __restrict__ cfg, float* __restrict__ conf, float* __restrict__ pz) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const float* y = Y + (size_t)i * O;
   const int m = raw[5 * (size_t)i], n = raw[5 * (size_t)i + 1];
+  const bool fok = (nullptr != fma_ok) && 0 != fma_ok[i];
   int best = 0;
   float ymax = -INFINITY;
   for (int c = 0; c < K; ++c) {
-    if (config_valid(c, m, n) && y[c] > ymax) {
+    if (config_valid(c, m, n, fok) && y[c] > ymax) {
       ymax = y[c];
       best = c;
     }
   }
   float z = 0.f;
   for (int c = 0; c < K; ++c) {
-    if (config_valid(c, m, n)) z += expf(y[c] - ymax);
+    if (config_valid(c, m, n, fok)) z += expf(y[c] - ymax);
   }
   cfg[i] = (unsigned char)best;
   conf[i] = 1.f / z;
@@ -390,19 +396,29 @@ int xs_mlp_predict(const float* weights, const int* raw, int N, unsigned char* c
   int r = set_smem_attrs();
   if (0 != r) return r;
   if (0 != (r = dev_alloc(d, N))) return r;
-  unsigned char* dcfg = nullptr;
-  r = (int)cudaMalloc(&dcfg, (size_t)N);
+  unsigned char *dcfg = nullptr, *dfma = nullptr;
+  /* where the FMA kernel takes the shape (host-side rule, the same one its launcher applies) */
+  unsigned char* const fma_ok = (unsigned char*)malloc((size_t)N);
+  if (nullptr == fma_ok) r = (int)cudaErrorMemoryAllocation;
+  else {
+    for (int i = 0; i < N; ++i) fma_ok[i] = (unsigned char)xs_smm_fma_supported(raw[5 * (size_t)i], raw[5 * (size_t)i + 1], raw[5 * (size_t)i + 2]);
+  }
+  if (0 == r) r = (int)cudaMalloc(&dcfg, (size_t)N);
+  if (0 == r) r = (int)cudaMalloc(&dfma, (size_t)N);
+  if (0 == r) r = (int)cudaMemcpy(dfma, fma_ok, (size_t)N, cudaMemcpyHostToDevice);
   if (0 == r) r = (int)cudaMemcpy(d.raw, raw, sizeof(int) * 5 * (size_t)N, cudaMemcpyHostToDevice);
   if (0 == r) r = (int)cudaMemcpy(d.W, weights, sizeof(float) * NW, cudaMemcpyHostToDevice);
   if (0 == r) {
     xs_mlp_fwd<<<(N + 127) / 128, 128, sizeof(float) * NW>>>(d.W, d.raw, N, d.X, d.H1, d.H2, d.Y);
-    xs_mlp_select<<<(N + 127) / 128, 128>>>(d.Y, d.raw, N, dcfg, d.loss, d.Z);
+    xs_mlp_select<<<(N + 127) / 128, 128>>>(d.Y, d.raw, dfma, N, dcfg, d.loss, d.Z);
     r = (int)cudaGetLastError();
   }
   if (0 == r) r = (int)cudaMemcpy(cfg, dcfg, (size_t)N, cudaMemcpyDeviceToHost);
   if (0 == r && nullptr != conf) r = (int)cudaMemcpy(conf, d.loss, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost);
   if (0 == r && nullptr != pz) r = (int)cudaMemcpy(pz, d.Z, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost);
   cudaFree(dcfg);
+  cudaFree(dfma);
+  free(fma_ok);
   dev_free(d);
   return r;
 }
@@ -465,8 +481,9 @@ void xs_mlp_uninstall(void) {
   pthread_mutex_unlock(&g_lock);
 }
 
-/* Predicted configuration for a shape from the installed table: returns 1 and fills mt, nt, kp and
-   the confidence (0..1) when a predictor is installed and the shape is inside the table, else 0. */
+/* Predicted configuration for a shape from the installed table: returns 1 and fills mt, nt, kp (kp =
+   XS_KP_FMA: the FMA kernel) and the confidence (0..1) when a predictor is installed and the shape is
+   inside the table, else 0. */
 int xs_mlp_lookup(int m, int n, int k, int S, int* mt, int* nt, int* kp, float* confidence) {
   int found = 0;
   if (m < 1 || n < 1 || k < 1 || m > kGridDim || n > kGridDim || k > kGridDim) return 0;
@@ -474,9 +491,9 @@ int xs_mlp_lookup(int m, int n, int k, int S, int* mt, int* nt, int* kp, float* 
   if (nullptr != g_cfg) {
     const size_t i = (((size_t)(m - 1) * kGridDim + (n - 1)) * kGridDim + (k - 1)) * kGridS + s_bucket(S);
     const int c = g_cfg[i];
-    *mt = (c >> 3) + 1;
-    *nt = ((c >> 1) & 3) + 1;
-    *kp = (c & 1) ? 4 : 2;
+    *mt = (kFmaConfig == c) ? 1 : (c >> 3) + 1;
+    *nt = (kFmaConfig == c) ? 1 : ((c >> 1) & 3) + 1;
+    *kp = (kFmaConfig == c) ? XS_KP_FMA : ((c & 1) ? 4 : 2);
     if (nullptr != confidence) *confidence = (float)g_conf[i] / 255.f;
     found = 1;
   }

@@ -18,16 +18,19 @@
  * Device layout: digit planes dA[s][M][Kp] and dB[s][N][Kp] (int8, K contiguous, Kp = K rounded
  * up to 16, zero padded), exponents ea[M], eb[N] (int32).
  *
- * GEMM kernel: one CTA per 128 x 256 tile of C, 6 warps. Warp 0 (one lane) streams (pair, k-block)
- * tiles of both operands into a 4-stage shared-memory ring with TMA (3-D tensor maps over the digit
- * planes, 128-byte swizzle, out-of-range rows and k read as zero); warp 1 owns 512 tensor-memory
- * columns (two 128 x 256 int32 accumulators) and one lane issues tcgen05.mma (M=128, N=256, K=32)
- * per 32-byte K step, committing each stage back to the producer and each finished diagonal to
- * the epilogue; warps 2-5 (one tensor-memory lane quarter each) read a finished accumulator with
- * tcgen05.ld, scale it and add it into C in FP64, then hand the accumulator back, so the tensor
- * cores work on diagonal d+1 while diagonal d is being recombined. Every mbarrier wait is bounded:
- * a stalled pipeline ends the kernel with an error status (per-call abort word and the library's
- * device error word) instead of a hang.
+ * GEMM kernel: one CTA per 128 x 128 tile of C, 6 warps. Warp 0 (one lane) streams (pair, k-block)
+ * tiles of both operands into a 6-stage shared-memory ring with TMA (3-D tensor maps over the digit
+ * planes, 128-byte swizzle, out-of-range rows and k read as zero); warp 1 owns all 512 tensor-memory
+ * columns -- two 128 x 128 int32 accumulators and the tile's FP64 partial sum (two 32-bit columns per
+ * C column) -- and one lane issues tcgen05.mma (M=128, N=128, K=32) per 32-byte K step, committing
+ * each stage back to the producer and each finished diagonal to the epilogue; warps 2-5 (one
+ * tensor-memory lane quarter each) read a finished accumulator with tcgen05.ld, scale it and add it
+ * in FP64 to the partial sum, which stays in tensor memory from diagonal to diagonal (tcgen05.st):
+ * C is read once (beta) at the first diagonal and written once at the last, instead of a
+ * read-modify-write of C per diagonal. The accumulator goes back to the MMA issuer after each
+ * diagonal, so the tensor cores work on diagonal d+1 while diagonal d is being recombined. Every
+ * mbarrier wait is bounded: a stalled pipeline ends the kernel with an error status (per-call abort
+ * word and the library's device error word) instead of a hang, leaving C unwritten.
  */
 #include "internal.h"
 #include "tc_ptx.cuh"
@@ -43,7 +46,8 @@ namespace {
 using namespace xs_tc;
 using namespace xs_oz;
 
-constexpr int kBM = 128, kBN = 256, kBK = 128, kStages = 4;
+constexpr int kBM = 128, kBN = 128, kBK = 128, kStages = 6;
+constexpr uint32_t kPartCol = 2 * kBN; /* tensor-memory column of the FP64 partial sum (2 columns per C column) */
 constexpr int kMaxSlices = 8;
 constexpr int kMaxPairs = kMaxSlices * kMaxSlices;
 constexpr int kMaxGroups = 2 * kMaxSlices - 1;
@@ -276,42 +280,63 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       }
     }
   }
-  else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4 */
+  else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; this lane's row of the tile keeps
+            its FP64 partial sum in tensor memory from one diagonal to the next */
     const int q = warp & 3;
     const int row = m0 + q * 32 + lane;
     const bool rok = row < args.M;
     const int ear = rok ? args.ea[row] : 0;
+    const uint32_t tlane = tmem + ((uint32_t)(q * 32) << 16);
+    const bool read_c = (0 == args.first) || 0.0 != args.beta;
     for (int g = 0; g < args.ngroups; ++g) {
       const int buf = g & 1, use = g >> 1;
       if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u, args.wait_limit)) break;
       tc_fence_after();
       const int eshift = args.g[g].eshift;
-      const bool beta_now = (0 != args.first) && (0 == g);
-      for (int c0 = 0; c0 < kBN; c0 += 32) {
-        uint32_t v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * kBN + c0), v);
+      const bool first_g = (0 == g), last_g = (g + 1 == args.ngroups);
+      for (int c0 = 0; c0 < kBN; c0 += 16) {
+        uint32_t v[16], pw[32];
+        tmem_ld16(tlane + (uint32_t)(buf * kBN + c0), v);
+        if (!first_g) tmem_ld32(tlane + kPartCol + (uint32_t)(2 * c0), pw);
         tmem_ld_wait();
-        if (rok) { /* all 32 loads of the chunk first, then the updates and the stores (no load waits for a
-                      store it cannot be proven independent of) */
-          double* const crow = args.C + row + (long long)(n0 + c0) * args.ldc;
-          const int ncol = min(32, args.N - (n0 + c0));
-          const bool read_c = !beta_now || 0.0 != args.beta;
-          double cv[32];
+        const int ncol = min(16, args.N - (n0 + c0));
+        double* const crow = args.C + row + (long long)(n0 + c0) * args.ldc;
+        double part[16];
+        if (first_g) { /* the partial sum starts as beta * C (the call's first launch) or C (a later K range) */
 #pragma unroll
-          for (int j = 0; j < 32; ++j) cv[j] = (j < ncol && read_c) ? crow[(long long)j * args.ldc] : 0.0;
+          for (int j = 0; j < 16; ++j) part[j] = (rok && j < ncol && read_c) ? crow[(long long)j * args.ldc] : 0.0;
+          if (0 != args.first) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            double c = beta_now ? args.beta * cv[j] : cv[j];
-            const int iv = (int)v[j];
-            if (0 != iv) c = add_scaled(c, iv, ear + s_eb[c0 + j] + eshift, args.alpha);
-            cv[j] = c;
-          }
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            if (j < ncol) crow[(long long)j * args.ldc] = cv[j];
+            for (int j = 0; j < 16; ++j) part[j] *= args.beta;
           }
         }
+        else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) part[j] = __hiloint2double((int)pw[2 * j + 1], (int)pw[2 * j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int iv = (int)v[j];
+          if (0 != iv) part[j] = add_scaled(part[j], iv, ear + s_eb[c0 + j] + eshift, args.alpha);
+        }
+        if (last_g) {
+          if (rok) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              if (j < ncol) crow[(long long)j * args.ldc] = part[j];
+            }
+          }
+        }
+        else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            pw[2 * j] = (uint32_t)__double2loint(part[j]);
+            pw[2 * j + 1] = (uint32_t)__double2hiint(part[j]);
+          }
+          tmem_st32(tlane + kPartCol + (uint32_t)(2 * c0), pw);
+        }
       }
+      if (!last_g) tmem_st_wait(); /* the partial sums are in tensor memory before the next diagonal reads them */
       tc_fence_before();
       mbar_arrive(&acce[buf]);
     }

@@ -1799,11 +1799,15 @@ cudaError_t launch_fma(const SmmPlan& pl, const StackTask& tk, int* seglist, con
 struct FmaEntry {
   int m, n, k; /* 0: runtime */
   int mmax, nmax;
-  int regs; /* accumulators per lane (RB * CB): the size of a piece is regs * 32 doubles */
+  int regs;  /* accumulators per lane (RB * CB): the size of a piece is regs * 32 doubles */
+  int D;     /* ring depth */
+  int slack; /* doubles after the last stage */
   launch_fn_t fn;
 };
-#define XS_FMA(M, N, K, LR, RB, CB, D) {M, N, K, M, N, RB * CB, &launch_fma<M, N, K, LR, RB, CB, D>}
-#define XS_FMA_RT(LR, RB, CB, D) {0, 0, 0, LR * RB, 32 / LR * CB, RB * CB, &launch_fma<0, 0, 0, LR, RB, CB, D>}
+#define XS_FMA(M, N, K, LR, RB, CB, D) \
+  {M, N, K, M, N, RB * CB, D, (32 / LR * CB + 1) / 2 * 2, &launch_fma<M, N, K, LR, RB, CB, D>}
+#define XS_FMA_RT(LR, RB, CB, D) \
+  {0, 0, 0, LR * RB, 32 / LR * CB, RB * CB, D, (32 / LR * CB + 1) / 2 * 2, &launch_fma<0, 0, 0, LR, RB, CB, D>}
 static const FmaEntry fma_table[] = {
   XS_FMA(4, 4, 4, 4, 1, 1, 8), XS_FMA(5, 5, 5, 8, 1, 2, 8), XS_FMA(6, 6, 18, 8, 1, 2, 6), XS_FMA(13, 4, 16, 16, 1, 2, 6),
   XS_FMA(32, 9, 9, 16, 2, 5, 4), XS_FMA(16, 64, 9, 8, 2, 16, 3), XS_FMA(7, 10, 5, 8, 1, 3, 8),
@@ -2209,14 +2213,9 @@ int xs_smm_f64_specialized(int m, int n, int k, int* mt_kp_pairs, int capacity) 
 int xs_smm_fma_supported(int m, int n, int k) {
   const FmaEntry* const f = find_fma(m, n, k);
   if (nullptr == f) return 0;
-  int occ = 0; /* the lane grid covers the block; the ring of the shape must also fit shared memory */
-  SmmPlan pl = {};
-  pl.W = 4;
-  StackTask tk = {};
-  tk.m = m;
-  tk.n = n;
-  tk.k = k;
-  return (cudaSuccess == f->fn(pl, tk, nullptr, nullptr, 0, &occ) && 0 < occ) ? 1 : 0;
+  /* the lane grid covers the block; its ring (4 warps per CTA) must also fit shared memory: the check
+     launch_fma makes, without a device call */
+  return (fma_smem_bytes(m, n, k, f->D, f->regs, f->slack, 4) <= 227 * 1024) ? 1 : 0;
 }
 
 size_t xs_smm_f64_scratch_bytes(int stack_size, int m, int n, int k, const xs_smm_params_t* params) {

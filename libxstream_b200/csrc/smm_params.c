@@ -128,9 +128,10 @@ void xs_params_lookup_ex(int type, int m, int n, int k, int stack_size, xs_smm_p
       xs_sanitize(out);
       if (NULL != source) *source = (conf >= xs_mlp_minconf()) ? XS_PARAMS_PREDICTED : XS_PARAMS_LOWCONF;
     }
-    { /* a staged kernel compiled for the shape (listed with kp = 0) beat the register kernel's
-         configurations where it was measured: its whole-block tile replaces heuristic and predicted
-         tiles (tuned records stay as recorded) */
+    if (XS_KP_FMA != out->kp) { /* a staged kernel compiled for the shape (listed with kp = 0) beat the
+         register kernel's configurations where it was measured: its whole-block tile replaces heuristic
+         and predicted DMMA tiles (tuned records and a predicted FMA kernel stay; the tuner times the
+         staged kernel under its whole-block tile, so the predictor learned it against the FMA kernel) */
       int triples[3 * 8], i;
       const int nspec = xs_smm_f64_specialized(m, n, k, triples, 8);
       for (i = 0; i < nspec && i < 8; ++i) {

@@ -1,9 +1,10 @@
 """Autotuner sweeps and the learned parameter predictor (host side).
 
 The exhaustive tuner (libxstream_b200_tune) times every precompiled configuration of the plain stack
-kernel -- tile class MT x NT (each <= ceil(dim/8), <= 4) and k-panel KP in {2, 4}, 32 classes
-c = (mt-1)*8 + (nt-1)*2 + (kp==4) -- and, for m, n, k <= 64, the Ozaki form, on synthetic stacks of a
-given shape and size. A sweep over many shapes is the predictor's training set: every (shape, stack
+kernels -- the DMMA tile classes MT x NT (each <= ceil(dim/8), <= 4) with k-panel KP in {2, 4}, 32
+classes c = (mt-1)*8 + (nt-1)*2 + (kp==4), and the register-blocked FMA kernel, c = 32, where its lane
+grids cover the block -- and, for m, n, k <= 64, the Ozaki form, on synthetic stacks of a given shape
+and size. A sweep over many shapes is the predictor's training set: every (shape, stack
 size) becomes samples for the exponent spreads {0, 10, 40} with targets r_c = t_c / t_best and the
 Ozaki label (Ozaki faster than the best plain configuration). The network (3 x FP32 width 64, see
 csrc/mlp.cu) is trained on the device by the library's own kernels; the exhaustive tuner is its
@@ -12,6 +13,8 @@ scored by the measured time of the predicted configuration against the tuned opt
 
 Command line (one GPU):
   python -m libxstream_b200.predictor sweep --out sweep.csv --shapes 4000 --heldout 300 --minutes 12
+  python -m libxstream_b200.predictor sweep --fma-only --out sweep_fma.csv   # re-tune the shapes the
+        FMA kernel takes, with every candidate; train/eval --override sweep_fma.csv replace those rows
   python -m libxstream_b200.predictor train --sweep sweep.csv --out mlp.txt
   python -m libxstream_b200.predictor eval --sweep sweep.csv --weights mlp.txt
 """
@@ -27,26 +30,44 @@ from pathlib import Path
 
 import numpy as np
 
-K = 32
+K = 33  # configurations: 32 DMMA tile classes, then the FMA kernel
+FMA = 32
 NFEAT = 27
 SPREADS = (0, 10, 40)
 SIZES = (1000, 10000, 100000)
 PARAMS_DIR = Path(__file__).resolve().parent / "params"
 DEFAULT_WEIGHTS = PARAMS_DIR / "mlp_b200.txt"
 DEFAULT_SWEEP = PARAMS_DIR / "sweep_b200.csv.gz"
+DEFAULT_SWEEP_FMA = PARAMS_DIR / "sweep_fma_b200.csv.gz"  # the FMA kernel's shapes re-tuned with every candidate
 
 
 def config_index(mt: int, nt: int, kp: int) -> int:
+    if kp < 0:  # the FMA kernel (kp = -1)
+        return FMA
     return (mt - 1) * 8 + (nt - 1) * 2 + (1 if kp == 4 else 0)
 
 
 def config_of(c: int) -> tuple[int, int, int]:
+    if c == FMA:
+        return 1, 1, -1
     return (c >> 3) + 1, ((c >> 1) & 3) + 1, 4 if (c & 1) else 2
 
 
-def valid_mask(m: int, n: int) -> np.ndarray:
+def fma_supported(m: int, n: int, k: int) -> bool:
+    """The FMA kernel takes m x n x k (its lane grids cover the block, its ring fits shared memory):
+    the library's own rule (a host function, no device call)."""
+    from . import lib as _lib
+    f = _lib().xs_smm_fma_supported
+    f.restype, f.argtypes = ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    return bool(f(m, n, k))
+
+
+def valid_mask(m: int, n: int, k: int | None = None) -> np.ndarray:
+    """Configurations that apply to m x n (x k): the DMMA tile classes up to ceil(dim/8) fragments,
+    the FMA kernel where it takes the shape (only when k is given)."""
     mtmax, ntmax = min(4, max(1, (m + 7) // 8)), min(4, max(1, (n + 7) // 8))
-    return np.array([config_of(c)[0] <= mtmax and config_of(c)[1] <= ntmax for c in range(K)])
+    v = [config_of(c)[0] <= mtmax and config_of(c)[1] <= ntmax for c in range(FMA)]
+    return np.array(v + [k is not None and fma_supported(m, n, k)])
 
 
 def random_shapes(count: int, seed: int, lo: int = 4, hi: int = 80, exclude: set | None = None) -> list[tuple[int, int, int]]:
@@ -71,19 +92,20 @@ def tune_one(lib, m: int, n: int, k: int, S: int, reps: int = 2, ozaki: int = 7,
     if got < nc:
         raise RuntimeError(f"tune {m}x{n}x{k} S={S} failed ({got}, last error {lib.libxstream_b200_last_error()})")
     out = {}
-    for i in range(nc):  # the DMMA tile classes by index; the FMA kernel (kp = -1) under "fma"
+    for i in range(nc):  # configuration index -> ms (the FMA kernel, kp = -1, is index FMA)
         if ms[i] < 0:
             continue  # the candidate does not take this shape
-        key = "fma" if cand[3 * i + 2] < 0 else config_index(cand[3 * i], cand[3 * i + 1], cand[3 * i + 2])
-        out[key] = float(ms[i])
+        out[config_index(cand[3 * i], cand[3 * i + 1], cand[3 * i + 2])] = float(ms[i])
     if got > nc:
         out["oz"] = float(ms[nc])
     return out
 
 
-def sweep(out: Path, shapes: list, heldout: list, minutes: float, reps: int = 2, header: bool = True) -> int:
+def sweep(out: Path, shapes: list, heldout: list, minutes: float, reps: int = 2, header: bool = True,
+          fma_only: bool = False) -> int:
     """Tunes held-out shapes first, then training shapes, until the time budget is spent; one CSV row
-    per (shape, stack size): split,m,n,k,S,t_0..t_31 (ms, empty = not applicable),t_oz."""
+    per (shape, stack size): split,m,n,k,S,t_0..t_32 (ms, empty = not applicable; t_32 is the FMA
+    kernel),t_oz. fma_only: only the shapes the FMA kernel takes (every candidate is still timed)."""
     from . import lib as _lib
     lib = _lib()
     t_end = time.time() + 60.0 * minutes
@@ -96,6 +118,8 @@ def sweep(out: Path, shapes: list, heldout: list, minutes: float, reps: int = 2,
             for (m, n, k) in group:
                 if time.time() > t_end:
                     break
+                if fma_only and not fma_supported(m, n, k):
+                    continue
                 for S in SIZES:
                     t = tune_one(lib, m, n, k, S, reps)
                     cells = [f"{t[c]:.5f}" if c in t else "" for c in range(K)]
@@ -105,21 +129,28 @@ def sweep(out: Path, shapes: list, heldout: list, minutes: float, reps: int = 2,
     return rows
 
 
-def load_sweep(path: Path) -> list[dict]:
+def load_sweep(path: Path, override: Path | None = None) -> list[dict]:
+    """Sweep records; a file with 32 configuration columns (before the FMA kernel) has no FMA time.
+    override: a second sweep whose rows replace the rows of the same (m, n, k, S)."""
     opener = gzip.open if str(path).endswith(".gz") else open
     recs = []
     with opener(path, "rt") as f:
-        next(f)
+        cols = next(f).rstrip("\n").split(",")
+        nk = sum(1 for c in cols if c.startswith("t") and c[1:].isdigit())
         for line in f:
             p = line.rstrip("\n").split(",")
-            t = np.array([float(x) if x else np.nan for x in p[5:5 + K]])
+            t = np.full(K, np.nan)
+            t[:nk] = [float(x) if x else np.nan for x in p[5:5 + nk]]
             recs.append({"split": p[0], "m": int(p[1]), "n": int(p[2]), "k": int(p[3]), "S": int(p[4]), "t": t,
-                         "oz": float(p[5 + K]) if p[5 + K] else None})
+                         "oz": float(p[5 + nk]) if p[5 + nk] else None})
+    if override is not None:
+        newer = {(r["m"], r["n"], r["k"], r["S"]): r for r in load_sweep(override)}
+        recs = [newer.pop((r["m"], r["n"], r["k"], r["S"]), r) for r in recs] + list(newer.values())
     return recs
 
 
 def build_dataset(recs: list[dict], spreads=SPREADS):
-    """raw (N, 5) int32, r (N, 32) float32 (t_c / t_best, 0 = not applicable), z (N,) float32."""
+    """raw (N, 5) int32, r (N, K) float32 (t_c / t_best, 0 = not applicable), z (N,) float32."""
     raw, r, z = [], [], []
     for rec in recs:
         t = rec["t"]
@@ -142,10 +173,12 @@ def nweights() -> int:
 
 
 def init_weights(seed: int = 7) -> np.ndarray:
-    """He-normal weights, zero biases (layout W1[F][64], b1, W2[64][64], b2, W3[64][33], b3)."""
+    """He-normal weights, zero biases (layout W1[F][64], b1, W2[64][64], b2, W3[64][K + 1], b3: K
+    configuration logits and the Ozaki logit)."""
     g = np.random.Generator(np.random.PCG64(seed))
+    out = K + 1
     parts = [g.normal(0, math.sqrt(2 / NFEAT), NFEAT * 64), np.zeros(64), g.normal(0, math.sqrt(2 / 64), 64 * 64), np.zeros(64),
-             g.normal(0, math.sqrt(1 / 64), 64 * 33), np.zeros(33)]
+             g.normal(0, math.sqrt(1 / 64), 64 * out), np.zeros(out)]
     return np.concatenate(parts).astype(np.float32)
 
 
@@ -158,6 +191,8 @@ def train(raw: np.ndarray, r: np.ndarray, z: np.ndarray, steps: int = 3000, lr: 
     """Trains on the device; returns (weights, loss per step)."""
     from . import lib as _lib
     w = (init_weights(seed) if weights is None else np.array(weights, dtype=np.float32)).copy()
+    if w.size != nweights():  # the device copies exactly nweights() floats in and out of w
+        raise ValueError(f"weights hold {w.size} floats, the network {nweights()}")
     hist = np.zeros(max(steps, 1), dtype=np.float32)
     rc = _lib().libxstream_b200_mlp_train(_ptr(raw), _ptr(r), _ptr(z), raw.shape[0], steps, lr, _ptr(w), _ptr(hist))
     if rc != 0:
@@ -271,23 +306,27 @@ def main(argv=None):
     s.add_argument("--seed", type=int, default=2025)
     s.add_argument("--start", type=int, default=0, help="first training shape (continue an earlier sweep)")
     s.add_argument("--no-heldout", action="store_true", help="skip the held-out shapes (tuned by an earlier sweep)")
+    s.add_argument("--fma-only", action="store_true", help="only the shapes the FMA kernel takes")
     t = sub.add_parser("train")
     t.add_argument("--sweep", type=Path, default=DEFAULT_SWEEP)
+    t.add_argument("--override", type=Path, default=DEFAULT_SWEEP_FMA, help="rows replacing the sweep's (none: '')")
     t.add_argument("--out", type=Path, default=DEFAULT_WEIGHTS)
     t.add_argument("--steps", type=int, default=3000)
     t.add_argument("--lr", type=float, default=3e-3)
     e = sub.add_parser("eval")
     e.add_argument("--sweep", type=Path, default=DEFAULT_SWEEP)
+    e.add_argument("--override", type=Path, default=DEFAULT_SWEEP_FMA, help="rows replacing the sweep's (none: '')")
     e.add_argument("--weights", type=Path, default=DEFAULT_WEIGHTS)
     e.add_argument("--minconf", type=float, default=0.0)
     a = ap.parse_args(argv)
     if a.cmd == "sweep":
         held = random_shapes(a.heldout, a.seed + 1)
         train_shapes = random_shapes(a.shapes, a.seed, exclude=set(held))
-        rows = sweep(a.out, train_shapes[a.start:], [] if a.no_heldout else held, a.minutes)
+        rows = sweep(a.out, train_shapes[a.start:], [] if a.no_heldout else held, a.minutes, fma_only=a.fma_only)
         print(json.dumps({"rows": rows, "out": str(a.out)}))
     elif a.cmd == "train":
-        recs = [r for r in load_sweep(a.sweep) if r["split"] == "train"]
+        ov = a.override if a.override and str(a.override) and Path(a.override).exists() else None
+        recs = [r for r in load_sweep(a.sweep, ov) if r["split"] == "train"]
         # choose steps / learning rate on a validation tenth of the training shapes, then retrain on all
         shapes = sorted({(r["m"], r["n"], r["k"]) for r in recs})
         g = np.random.Generator(np.random.PCG64(99))
@@ -308,7 +347,8 @@ def main(argv=None):
         print(json.dumps({"samples": int(raw.shape[0]), "search": search, "chosen": best, "loss_first": float(hist[0]),
                           "loss_last": float(hist[-1]), "out": str(a.out)}))
     else:
-        recs = [r for r in load_sweep(a.sweep) if r["split"] == "heldout"]
+        ov = a.override if a.override and str(a.override) and Path(a.override).exists() else None
+        recs = [r for r in load_sweep(a.sweep, ov) if r["split"] == "heldout"]
         w = load_weights(a.weights)
         print(json.dumps(evaluate(recs, lambda raw: device_predict(w, raw), minconf=a.minconf)))
 

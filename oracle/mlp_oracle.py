@@ -3,8 +3,9 @@ features, forward pass, loss and gradients as the device kernels in libxstream_b
 that the device's forward pass and gradients can be checked against it (and it against finite
 differences).
 
-Network: 27 features -> relu(64) -> relu(64) -> 33 outputs (32 configuration logits + 1 Ozaki logit).
-Weights are one flat vector: W1[27][64], b1[64], W2[64][64], b2[64], W3[64][33], b3[33].
+Network: 27 features -> relu(64) -> relu(64) -> 34 outputs (33 configuration logits: 32 DMMA tile
+classes and the FMA kernel, + 1 Ozaki logit).
+Weights are one flat vector: W1[27][64], b1[64], W2[64][64], b2[64], W3[64][34], b3[34].
 Loss per sample: cross-entropy of the masked softmax of the configuration logits against the soft
 target q_c ~ exp(-(r_c - 1) / 0.02) over the applicable configurations (r_c > 0), plus the binary
 cross-entropy of the Ozaki logit when its label z is 0 or 1; the total is the mean.
@@ -13,7 +14,7 @@ from __future__ import annotations
 
 import numpy as np
 
-F, H, K = 27, 64, 32
+F, H, K = 27, 64, 33
 TARGET_TEMP = 0.02
 O = K + 1
 SHAPES = [("W1", (F, H)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("W3", (H, O)), ("b3", (O,))]
@@ -95,14 +96,18 @@ def loss_and_grad(w: np.ndarray, raw: np.ndarray, r: np.ndarray, z: np.ndarray):
     return float(losses.mean()), losses, pack(g)
 
 
-def predict(w: np.ndarray, raw: np.ndarray):
-    """Masked argmax configuration, its softmax probability and the Ozaki probability."""
+def predict(w: np.ndarray, raw: np.ndarray, fma_ok: np.ndarray | None = None):
+    """Masked argmax configuration, its softmax probability and the Ozaki probability. The DMMA tile
+    classes (c < 32) apply up to ceil(dim/8) fragments; the FMA kernel (c = 32) where fma_ok (per
+    sample, the library's rule for its lane grids and ring; None: nowhere)."""
     _, _, _, y = forward(w, raw)
     raw = np.asarray(raw)
     mtmax = np.clip((raw[:, 0] + 7) // 8, 1, 4)
     ntmax = np.clip((raw[:, 1] + 7) // 8, 1, 4)
     c = np.arange(K)
-    valid = ((c[None, :] >> 3) + 1 <= mtmax[:, None]) & ((((c[None, :] >> 1) & 3) + 1) <= ntmax[:, None])
+    valid = ((c[None, :] >> 3) + 1 <= mtmax[:, None]) & ((((c[None, :] >> 1) & 3) + 1) <= ntmax[:, None]) & (c[None, :] < 32)
+    fok = np.zeros(raw.shape[0], dtype=bool) if fma_ok is None else np.asarray(fma_ok, dtype=bool)
+    valid[:, 32] = fok
     yc = np.where(valid, y[:, :K], -np.inf)
     best = yc.argmax(axis=1)
     e = np.where(valid, np.exp(yc - yc.max(axis=1, keepdims=True)), 0.0)

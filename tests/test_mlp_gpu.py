@@ -73,7 +73,8 @@ def test_predict_kernel_matches_oracle(acc):
     w = P.init_weights(11) * 2.0
     raw, _, _ = random_problem(500, 4)
     cfg, conf, pz = P.device_predict(w, raw)
-    rcfg, rconf, rpz = M.predict(w.astype(np.float64), raw)
+    fma_ok = np.array([P.fma_supported(int(m), int(n), int(k)) for m, n, k in raw[:, :3]])
+    rcfg, rconf, rpz = M.predict(w.astype(np.float64), raw, fma_ok)
     assert np.mean(cfg == rcfg) >= 0.995  # ties within FP32 rounding may differ
     assert np.max(np.abs(conf - rconf)) <= 1e-4 and np.max(np.abs(pz - rpz)) <= 1e-4
 
@@ -89,12 +90,12 @@ def test_install_drives_parameter_lookup(acc):
             conf = ctypes.c_float()
             assert lib.libxstream_b200_mlp_lookup(m, n, k, S, out, ctypes.byref(conf)) == 1
             bucket = 1000 if S < 3000 else (10000 if S < 30000 else 100000)
-            rc, _, _ = M.predict(w.astype(np.float64), np.array([[m, n, k, bucket, 0]]))
+            rc, _, _ = M.predict(w.astype(np.float64), np.array([[m, n, k, bucket, 0]]), [P.fma_supported(m, n, k)])
             assert P.config_index(out[0], out[1], out[2]) == int(rc[0])
             p6 = (ctypes.c_int * 6)()
             lib.libxstream_b200_get_params(m, n, k, S, p6)
-            if (m, n, k) == (23, 23, 23):  # a staged kernel exists: its whole-block tile is used instead
-                assert (p6[1], p6[2], p6[3]) == (3, 3, 0)
+            if (m, n, k) == (23, 23, 23) and int(rc[0]) != P.FMA:  # a staged kernel exists: its whole-block
+                assert (p6[1], p6[2], p6[3]) == (3, 3, 0)                # tile replaces a predicted DMMA tile
             else:
                 assert (p6[1], p6[2], p6[3]) == (out[0], out[1], out[2])
     finally:
@@ -110,5 +111,5 @@ def test_tuner_times_every_candidate(acc):
     cand = (ctypes.c_int * (3 * (P.K + 1)))()
     nc = lib.libxstream_b200_tune_candidates(20, 9, cand, P.K + 1)
     assert nc == 3 * 2 * 2 + 1 and len([c for c in t if c != "oz"]) == nc  # 12 DMMA tile classes + the FMA kernel
-    assert (cand[3 * 12], cand[3 * 12 + 1], cand[3 * 12 + 2]) == (1, 1, -1) and "fma" in t
+    assert (cand[3 * 12], cand[3 * 12 + 1], cand[3 * 12 + 2]) == (1, 1, -1) and P.FMA in t
     assert all(v > 0 for v in t.values()) and "oz" in t

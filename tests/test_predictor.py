@@ -46,10 +46,36 @@ def test_dataset_from_sweep(tmp_path):
     assert list(z[:3]) == [1.0, 1.0, 1.0] and list(z[3:]) == [-1.0, -1.0, -1.0]
 
 
+def test_initial_weights_match_the_network():
+    """The host weight vector has exactly the library's weight count (the device copies that many
+    floats in and out of it) and the oracle's."""
+    assert P.init_weights(3).size == P.nweights() == M.NW
+
+
 def test_config_index_roundtrip_and_masks():
     for c in range(P.K):
         assert P.config_index(*P.config_of(c)) == c
     assert P.valid_mask(8, 8).sum() == 2 and P.valid_mask(80, 80).sum() == 32 and P.valid_mask(20, 9).sum() == 12
+    # the FMA kernel (configuration 32) where its lane grids cover the block and its ring fits
+    assert P.valid_mask(8, 8, 8)[P.FMA] and P.valid_mask(20, 9, 13).sum() == 13 and P.valid_mask(16, 64, 9)[P.FMA]
+    assert not P.valid_mask(80, 80, 80)[P.FMA] and not P.valid_mask(33, 8, 8)[P.FMA]
+
+
+def test_sweep_without_fma_column_and_override(tmp_path):
+    """A sweep written before the FMA kernel (32 configuration columns) reads with no FMA time; rows of
+    an override sweep replace the rows of the same shape and size."""
+    old, new = tmp_path / "old.csv", tmp_path / "new.csv"
+    with open(old, "w") as f:
+        f.write("split,m,n,k,S," + ",".join(f"t{c}" for c in range(32)) + ",t_oz\n")
+        f.write("train,8,8,8,1000,0.2," + ",".join("" for _ in range(31)) + ",\n")
+        f.write("train,9,9,9,1000,0.3," + ",".join("" for _ in range(31)) + ",\n")
+    with open(new, "w") as f:
+        f.write("split,m,n,k,S," + ",".join(f"t{c}" for c in range(P.K)) + ",t_oz\n")
+        f.write("train,8,8,8,1000,0.25," + ",".join("" for _ in range(31)) + ",0.1,\n")
+    recs = P.load_sweep(old)
+    assert len(recs) == 2 and len(recs[0]["t"]) == P.K and np.isnan(recs[0]["t"][P.FMA])
+    recs = P.load_sweep(old, new)
+    assert len(recs) == 2 and recs[0]["t"][0] == 0.25 and recs[0]["t"][P.FMA] == 0.1 and recs[1]["t"][0] == 0.3
 
 
 @pytest.mark.skipif(not (P.DEFAULT_SWEEP.exists() and P.DEFAULT_WEIGHTS.exists()), reason="no committed sweep/weights")
@@ -58,12 +84,16 @@ def test_trained_predictor_beats_default_on_heldout_shapes():
     time of its choice: closer to the tuned optimum than the default heuristic (the method without
     the network), and within 5% of the optimum on most shapes; the exhaustive tuner as fallback for
     unconfident predictions brings every remaining shape to the optimum."""
-    recs = [r for r in P.load_sweep(P.DEFAULT_SWEEP) if r["split"] == "heldout"]
+    override = P.DEFAULT_SWEEP_FMA if P.DEFAULT_SWEEP_FMA.exists() else None
+    recs = [r for r in P.load_sweep(P.DEFAULT_SWEEP, override) if r["split"] == "heldout"]
     assert len(recs) >= 300
     w = P.load_weights(P.DEFAULT_WEIGHTS).astype(np.float64)
-    stats = P.evaluate(recs, lambda raw: M.predict(w, raw))
+
+    def predict(raw):  # the oracle's forward pass; the FMA kernel applies where the library's rule says
+        return M.predict(w, raw, [P.fma_supported(int(m), int(n), int(k)) for m, n, k in np.asarray(raw)[:, :3]])
+    stats = P.evaluate(recs, predict)
     assert stats["geomean_ratio"] < stats["default_geomean_ratio"]
     assert stats["within_5pct"] >= stats["default_within_5pct"] + 0.5  # measured: 0.96 vs 0.30
     assert stats["within_5pct"] >= 0.9
-    fb = P.evaluate(recs, lambda raw: M.predict(w, raw), minconf=0.5)
+    fb = P.evaluate(recs, predict, minconf=0.5)
     assert fb["within_5pct"] >= 0.97 and fb["fallback_rate"] <= 0.4  # measured: 0.99 with 31% tuned
