@@ -28,6 +28,7 @@
 #include "../../include/libxstream_b200.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 namespace {
@@ -153,7 +154,32 @@ struct StackTask {
   double alpha;   /* C += alpha * A * B (1 for the LIBSMM ABI) */
   int* arrive;    /* per (CTA group, sub-tile) arrival counters of CTA-crossing segments, zero at launch:
                      the stack kernel combines them itself; nullptr: they go to the combine kernel */
+  const int* raw; /* the caller's parameter stack (input of the grouping), for the L2 prefetch */
+  int rstride;    /* ints per parameter record (3 or 6) */
+  int rbase;      /* a-offset position within a record (b follows) */
+  int rshift;     /* added to a record's offsets to make them 0-based (-1: 1-based, 0: 0-based) */
+  int npf;        /* records whose A and B blocks are prefetched into L2 (0: none) */
 };
+
+/* Bulk prefetch into L2 of the A and B blocks of the first tk.npf parameter records, spread over the
+   grid's threads. It reads only the caller's inputs (the raw stack and the pools), so a stack kernel
+   runs it before pdl_wait, while the grouping that precedes it in the stream still runs and the
+   pools would otherwise be fetched only at the first copy. A block's window is widened to 16-byte
+   boundaries (the bulk-copy granule); a widened window never leaves the block's page. */
+__device__ __forceinline__ void prefetch_block(const double* p, uint32_t bytes) {
+  const uint64_t s = (uint64_t)p, s0 = s & ~15ull, s1 = (s + bytes + 15ull) & ~15ull;
+  xs_tc::bulk_prefetch_l2((const void*)s0, (uint32_t)(s1 - s0));
+}
+__device__ __forceinline__ void prefetch_operands(const StackTask& tk) {
+  if (0 >= tk.npf) return;
+  const uint32_t abytes = (uint32_t)(tk.m * tk.k * sizeof(double)), bbytes = (uint32_t)(tk.k * tk.n * sizeof(double));
+  const int nthreads = (int)(gridDim.x * blockDim.x);
+  for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < tk.npf; i += nthreads) {
+    const int* const e = tk.raw + (size_t)tk.rstride * i + tk.rbase;
+    prefetch_block(tk.a + (e[0] + tk.rshift), abytes);
+    prefetch_block(tk.b + (e[1] + tk.rshift), bbytes);
+  }
+}
 
 template <int MT, int NT>
 __device__ __forceinline__ void DmmaLayout<MT, NT>::commit(const StackTask& tk, int sub, size_t coff, const double (&sum)[REGS]) {
@@ -580,6 +606,7 @@ template <int M_, int N_, int K_, int MT, int NT, int KP>
 __global__ void __launch_bounds__(128, smm_min_blocks(MT, NT))
   xs_smm_dmma_kernel(const __grid_constant__ StackTask tk, int* __restrict__ seglist, const unsigned* __restrict__ err) {
   extern __shared__ double smem[];
+  prefetch_operands(tk);
   pdl_wait();
   pdl_trigger();
   if (0 != *(volatile const unsigned*)err) return; /* the grouping failed: write nothing */
@@ -707,6 +734,12 @@ __device__ __forceinline__ bool staged_item(const StackTask& tk, int group, int*
     if (p0 + 32 + lane < p1) {
       kn = keys[p0 + 32 + lane];
       vn = vals[p0 + 32 + lane];
+    }
+    { /* the C blocks of the segments that start in the first 64 entries go to L2 now, so that their
+         read-modify-write at the segment's end hits L2 */
+      const unsigned pc = __shfl_up_sync(FULL, kc, 1), pn = __shfl_up_sync(FULL, kn, 1), c31 = __shfl_sync(FULL, kc, 31);
+      if (p0 + lane < p1 && (0 == lane || pc != kc)) prefetch_block(tk.c + (kc - 1u), (uint32_t)(M_ * N_ * 8));
+      if (p0 + 32 + lane < p1 && ((0 == lane) ? c31 : pn) != kn) prefetch_block(tk.c + (kn - 1u), (uint32_t)(M_ * N_ * 8));
     }
     auto key_of = [&](int e) -> unsigned { /* e - wb in [0, 64) */
       const int i = e - wb;
@@ -881,6 +914,7 @@ __global__ void __launch_bounds__(128, smm_min_blocks((M_ + 7) / 8, (N_ + 7) / 8
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ int s_probe[2];
   __shared__ int duty[2][6];
+  prefetch_operands(tk);
   pdl_wait();
   pdl_trigger();
   if (0 != *(volatile const unsigned*)err) return;
@@ -943,6 +977,7 @@ __global__ void __launch_bounds__(32 * (NC + 1), MINB)
     meta[warp * 4 + 2] = 0;
     meta[warp * 4 + 3] = 0;
   }
+  prefetch_operands(tk);
   pdl_wait();
   pdl_trigger();
   if (__syncthreads_or((0 != *(volatile const unsigned*)err) ? 1 : 0)) return; /* the grouping failed: write nothing */
@@ -1224,6 +1259,7 @@ __global__ void __launch_bounds__(128, 2)
   constexpr unsigned FULL = 0xFFFFFFFFu;
   extern __shared__ __align__(16) double fsm[];
   __shared__ int s_probe[2];
+  prefetch_operands(tk);
   pdl_wait();
   pdl_trigger();
   if (__syncthreads_or((0 != *(volatile const unsigned*)err) ? 1 : 0)) return;
@@ -1555,6 +1591,7 @@ __global__ void __launch_bounds__(32 * kUniW, kUniMinBlocks)
   uint64_t* const bars = (uint64_t*)smraw;
   int* const meta = (int*)(smraw + kUniW * kUniR * sizeof(uint64_t));
   unsigned char* const area = smraw + kUniHeader;
+  for (int ti = 0; ti < bt.ntasks; ++ti) prefetch_operands(bt.t[ti]);
   pdl_wait();
   pdl_trigger();
   if (__syncthreads_or((0 != *(volatile const unsigned*)err) ? 1 : 0)) return;
@@ -2230,6 +2267,28 @@ int xs_launch_smm_f64(const int* dev_stack, int S, const double* a, const double
   return xs_launch_smm_f64_ex(dev_stack, S, 0, 1.0, a, b, c, m, n, k, prm, scratch, scratch_bytes, stream);
 }
 
+/* Operand bytes (A and B blocks, counted per parameter record) that a stack kernel prefetches into L2
+   while the grouping runs: 64 MB, about half the L2, so that the prefetched blocks are not evicted
+   before they are used; LIBXSTREAM_B200_PREFETCH_MB overrides it (0: no prefetch). */
+static long long prefetch_budget() {
+  static const long long v = []() -> long long {
+    const char* const env = getenv("LIBXSTREAM_B200_PREFETCH_MB");
+    const long long mb = (nullptr != env) ? atoll(env) : 64;
+    return (0 < mb) ? (mb << 20) : 0;
+  }();
+  return v;
+}
+
+/* Sets the prefetch fields of tk: the first records of the stack whose A and B blocks fit the budget. */
+static void set_prefetch(StackTask& tk, const int* dev_stack, int S, int format, long long budget) {
+  const long long per = (long long)tk.k * (tk.m + tk.n) * (long long)sizeof(double);
+  tk.raw = dev_stack;
+  tk.rstride = (0 != format) ? 6 : 3;
+  tk.rbase = (0 != format) ? 3 : 0;
+  tk.rshift = (0 != format) ? 0 : -1;
+  tk.npf = (0 < per) ? (int)((budget / per < S) ? budget / per : S) : 0;
+}
+
 int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, const double* a, const double* b, double* c,
   int m, int n, int k, const xs_smm_params_t* prm, void* scratch, size_t scratch_bytes, void* stream) {
   SmmPlan pl;
@@ -2278,6 +2337,7 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   tk.nsub_n = pl.nsub_n;
   tk.nsub = pl.nsub;
   tk.arrive = arrive; /* CTA-crossing segments are combined inside the stack kernel */
+  set_prefetch(tk, dev_stack, S, format, prefetch_budget());
   const launch_fn_t fn = find_launcher(m, n, k, prm);
   return (int)fn(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
 }
@@ -2347,7 +2407,13 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
   /* task table in item order (heaviest items first) */
   BatchTasks bt;
   memset(&bt, 0, sizeof(bt));
-  double flops = 0, bytes = 0;
+  double flops = 0, bytes = 0, pf_total = 0;
+  for (int i = 0; i < up.nparts; ++i) {
+    const libxstream_b200_stack_t& d = st[up.part[i].stack];
+    pf_total += 8.0 * d.k * (double)(d.m + d.n) * up.part[i].S;
+  }
+  /* the prefetch budget is shared by the parts in proportion to their operand bytes */
+  const double pf_scale = (pf_total > (double)prefetch_budget()) ? (double)prefetch_budget() / pf_total : 1.0;
   for (int i = 0; i < up.nparts; ++i) {
     const int q = up.order[i];
     const UniPart& p = up.part[q];
@@ -2374,6 +2440,8 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     tk.kind = p.kind;
     tk.sid = q;
     tk.item_begin = bt.nitems;
+    set_prefetch(tk, d.dev_param_stack + 3 * (size_t)p.first, p.S, 0,
+      (long long)(pf_scale * 8.0 * d.k * (double)(d.m + d.n) * p.S));
     bt.t[bt.ntasks++] = tk;
     bt.nitems += p.ngroups * p.nsub;
     flops += 2.0 * d.m * d.n * d.k * (double)p.S;

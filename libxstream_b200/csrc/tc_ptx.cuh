@@ -112,6 +112,12 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
     : "memory");
 }
 
+/* 1-D bulk prefetch of global memory into L2 (16-byte aligned address, size a multiple of 16); no
+   completion to wait for. */
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)map) : "memory");
 }
