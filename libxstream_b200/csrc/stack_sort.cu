@@ -119,6 +119,27 @@ __device__ __forceinline__ unsigned div_floor(unsigned x, unsigned d, unsigned m
   return q;
 }
 
+/* For each of this lane's E digits, the lanes of the warp holding the same digit (what
+   __match_any_sync returns), from one ballot per digit bit: bits 0..nbits-1 and bit kRadixBits, which
+   only the no-entry digit kRadix sets. Ballots cost far less than match instructions. */
+template <int E>
+__device__ __forceinline__ void match_digits(const int (&dig)[E], int nbits, unsigned (&peers)[E]) {
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const bool x = 0 != ((dig[r] >> kRadixBits) & 1);
+    const unsigned v = __ballot_sync(0xffffffffu, x);
+    peers[r] = x ? v : ~v;
+  }
+  for (int b = 0; b < nbits; ++b) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const bool x = 0 != ((dig[r] >> b) & 1);
+      const unsigned v = __ballot_sync(0xffffffffu, x);
+      peers[r] &= x ? v : ~v;
+    }
+  }
+}
+
 /* Block-wide exclusive scan of R values held PER per thread (thread i owns [i*PER, (i+1)*PER));
    returns the block total. */
 template <int PER>
@@ -333,10 +354,13 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
       if ((j & (kRadix - 1)) < R) (&s_wc[0][0])[j] = 0;
     }
     __syncthreads();
+    { /* one shared-memory add per distinct digit of a warp round (hot C blocks) */
+      unsigned pr[E];
+      match_digits<E>(dig, rb, pr);
 #pragma unroll
-    for (int r = 0; r < E; ++r) { /* one shared-memory add per distinct digit of a warp round (hot C blocks) */
-      const unsigned pr = __match_any_sync(0xffffffffu, dig[r]);
-      if (kRadix != dig[r] && 0 == __popc(pr & ((1u << lane) - 1u))) atomicAdd(&s_base[dig[r]], __popc(pr));
+      for (int r = 0; r < E; ++r) {
+        if (kRadix != dig[r] && 0 == __popc(pr[r] & ((1u << lane) - 1u))) atomicAdd(&s_base[dig[r]], __popc(pr[r]));
+      }
     }
     __syncthreads();
     for (int d = threadIdx.x; d < R; d += blockDim.x) hist[(size_t)tile * kRadix + d] = s_base[d];
@@ -445,9 +469,9 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     if (0 == pass) XS_STAMP(5);
     /* (c) stable scatter: per-warp counts -> per-warp offsets -> ordered placement */
     unsigned peers[E];
+    match_digits<E>(dig, rb, peers);
 #pragma unroll
     for (int r = 0; r < E; ++r) {
-      peers[r] = __match_any_sync(0xffffffffu, dig[r]);
       if (kRadix != dig[r] && 0 == __popc(peers[r] & ((1u << lane) - 1u))) {
         s_wc[warp][dig[r]] += (unsigned short)__popc(peers[r]);
       }
@@ -525,17 +549,24 @@ template <int E>
 __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(const int* __restrict__ stack, int S, int format,
   unsigned blk, unsigned* __restrict__ k0, unsigned long long* __restrict__ v0, unsigned* __restrict__ k1,
   unsigned long long* __restrict__ v1, unsigned* __restrict__ kout, unsigned long long* __restrict__ vout,
-  int* __restrict__ seglist, int* __restrict__ zero, int nzero, SortCtl* ctl, int heavy) {
+  int* __restrict__ seglist, int* __restrict__ zero, int nzero, SortCtl* ctl, int heavy, unsigned blk_magic,
+  unsigned long long* __restrict__ stamps) {
   namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char s_dyn[];
   unsigned short (*const s_wc)[kRadix] = reinterpret_cast<unsigned short (*)[kRadix]>(s_dyn);
   int (*const s_all)[kRadix] = reinterpret_cast<int (*)[kRadix]>(s_dyn + sizeof(unsigned short) * kClWarps * kRadix);
-  __shared__ int s_base[kRadix]; /* digit write positions of this CTA */
+  __shared__ __align__(16) int s_base[kRadix]; /* digit write positions of this CTA */
   __shared__ int s_wsum[kClWarps];
   __shared__ unsigned s_red[3][kClWarps];
   __shared__ unsigned s_stat[kClusterMax][3]; /* cmin, cmax, gcd of every CTA, pushed by each */
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
+  /* optional phase timestamps (stamps != nullptr): [rank][8] */
+#define XS_CSTAMP(slot) \
+  do { \
+    if (nullptr != stamps && 0 == threadIdx.x) stamps[rank * 8 + (slot)] = global_ns(); \
+  } while (0)
+  XS_CSTAMP(0);
   asm volatile("griddepcontrol.launch_dependents;" :::);
   /* every CTA of the cluster must be running before another one writes into its shared memory: arrive
      now, wait before the first push (the stack loads overlap the barrier) */
@@ -595,6 +626,7 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
       }
       gg = __shfl_sync(0xffffffffu, gg, 0);
     }
+    XS_CSTAMP(1);
     asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
     if (0 == warp && lane < ncta) { /* push this CTA's statistics to every CTA of the cluster */
       unsigned* const st = cluster.map_shared_rank(&s_stat[rank][0], lane);
@@ -604,13 +636,17 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
     }
   }
   cluster.sync();
-  unsigned cmin = 0xFFFFFFFFu, cmax = 0u, g = blk;
-  for (int q = 0; q < ncta; ++q) { /* every thread combines the cluster's statistics (same order) */
-    cmin = min(cmin, s_stat[q][0]);
-    cmax = max(cmax, s_stat[q][1]);
-    if (0 == blk) g = gcd_acc(g, s_stat[q][2]);
+  XS_CSTAMP(2);
+  /* every warp combines the cluster's statistics, lane q taking CTA q's (ncta <= 16 < 32) */
+  const unsigned cmin = __reduce_min_sync(0xffffffffu, (lane < ncta) ? s_stat[lane][0] : 0xFFFFFFFFu);
+  const unsigned cmax = __reduce_max_sync(0xffffffffu, (lane < ncta) ? s_stat[lane][1] : 0u);
+  unsigned g = blk, gm = blk_magic; /* blk > 0: floor(2^32 / blk) from the host */
+  if (0 == blk) {
+    g = (lane < ncta) ? s_stat[lane][2] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) g = gcd_acc(g, __shfl_xor_sync(0xffffffffu, g, o));
+    gm = (1u < g) ? (unsigned)((1ull << 32) / g) : 0u;
   }
-  const unsigned gm = (1u < g) ? (unsigned)((1ull << 32) / g) : 0u;
   const unsigned nb = (0 == g) ? 1u : div_floor(cmax - cmin, g, gm) + 1u;
   int bits = 0;
   while (bits < 32 && (nb - 1u) >> bits) ++bits;
@@ -646,8 +682,7 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
     else if ((int)threadIdx.x < kClWarps * R) s_wc[threadIdx.x / R][threadIdx.x % R] = 0;
     __syncthreads();
     unsigned peers[E];
-#pragma unroll
-    for (int r = 0; r < E; ++r) peers[r] = __match_any_sync(0xffffffffu, dig[r]);
+    match_digits<E>(dig, rb, peers);
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       if (kRadix != dig[r] && 0 == __popc(peers[r] & ((1u << lane) - 1u))) {
@@ -656,58 +691,69 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
       __syncwarp();
     }
     __syncthreads();
-    /* (b) per digit: exclusive prefix over the warps in place; the CTA total goes to every CTA */
-    for (int d = threadIdx.x; d < R; d += kClThreads) {
-      int run = 0;
+    if (0 == pass) XS_CSTAMP(3);
+    /* (b) per digit: exclusive prefix over the warps in place; the CTA's totals go to every CTA.
+       Thread i owns the four digits [4i, 4i + 4) here and in (c), read and written as vectors
+       (counts < 2^16: a CTA holds kClThreads * E entries); digits >= R are never used. */
+    static_assert(kRadix == 4 * kClThreads, "four digits per thread");
+    const int d4 = 4 * (int)threadIdx.x;
+    if (d4 < R) {
+      unsigned run0 = 0u, run1 = 0u, run2 = 0u, run3 = 0u;
 #pragma unroll
       for (int w2 = 0; w2 < kClWarps; ++w2) {
-        const int c = s_wc[w2][d];
-        s_wc[w2][d] = (unsigned short)run;
-        run += c;
+        uint2* const p = reinterpret_cast<uint2*>(&s_wc[w2][d4]);
+        const uint2 c = *p;
+        *p = make_uint2(run0 | (run1 << 16), run2 | (run3 << 16));
+        run0 += c.x & 0xFFFFu;
+        run1 += c.x >> 16;
+        run2 += c.y & 0xFFFFu;
+        run3 += c.y >> 16;
       }
-      for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(&s_all[rank][d], q) = run;
+      const int4 t4 = make_int4((int)run0, (int)run1, (int)run2, (int)run3);
+      for (int q = 0; q < ncta; ++q) *cluster.map_shared_rank(reinterpret_cast<int4*>(&s_all[rank][d4]), q) = t4;
     }
     cluster.sync();
+    if (0 == pass) XS_CSTAMP(4);
     /* (c) write positions: exclusive scan of the cluster totals over the digits plus the counts of
-       the CTAs before this one. Thread i owns digits [i*per, (i+1)*per). */
-    constexpr int PER = kRadix / kClThreads;
-    const int per = (R + kClThreads - 1) / kClThreads;
-    int tot[PER], pre[PER];
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-      const int d = threadIdx.x * per + j;
-      int x = 0, p = 0;
-      if (j < per && d < R) {
-        for (int q = 0; q < ncta; ++q) {
-          const int c = s_all[q][d];
-          x += c;
-          p += (q < rank) ? c : 0;
+       the CTAs before this one. */
+    int tot[4] = {0, 0, 0, 0}, pre[4] = {0, 0, 0, 0};
+    if (d4 < R) {
+      for (int q = 0; q < ncta; ++q) {
+        const int4 c = *reinterpret_cast<const int4*>(&s_all[q][d4]);
+        tot[0] += c.x;
+        tot[1] += c.y;
+        tot[2] += c.z;
+        tot[3] += c.w;
+        if (q < rank) {
+          pre[0] += c.x;
+          pre[1] += c.y;
+          pre[2] += c.z;
+          pre[3] += c.w;
         }
       }
-      tot[j] = x;
-      pre[j] = p;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (d4 + j >= R) tot[j] = pre[j] = 0;
+      }
     }
     if (1 == passes && 0 < heavy) { /* C blocks with >= heavy entries first, then the rest; id order within each */
-      int hv[PER];
-      bool isheavy[PER];
+      int hv[4];
+      bool isheavy[4];
 #pragma unroll
-      for (int j = 0; j < PER; ++j) {
+      for (int j = 0; j < 4; ++j) {
         isheavy[j] = tot[j] >= heavy;
         hv[j] = isheavy[j] ? tot[j] : 0;
         tot[j] -= hv[j];
       }
-      const int nheavy = block_exscan<PER>(hv, s_wsum);
-      block_exscan<PER>(tot, s_wsum);
+      const int nheavy = block_exscan<4>(hv, s_wsum);
+      block_exscan<4>(tot, s_wsum);
 #pragma unroll
-      for (int j = 0; j < PER; ++j) tot[j] = isheavy[j] ? hv[j] : nheavy + tot[j];
+      for (int j = 0; j < 4; ++j) tot[j] = isheavy[j] ? hv[j] : nheavy + tot[j];
     }
-    else block_exscan<PER>(tot, s_wsum);
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-      const int d = threadIdx.x * per + j;
-      if (j < per && d < R) s_base[d] = tot[j] + pre[j];
-    }
+    else block_exscan<4>(tot, s_wsum);
+    if (d4 < R) *reinterpret_cast<int4*>(&s_base[d4]) = make_int4(tot[0] + pre[0], tot[1] + pre[1], tot[2] + pre[2], tot[3] + pre[3]);
     __syncthreads();
+    if (0 == pass) XS_CSTAMP(5);
     /* (d) stable placement in stack order: CTA base + warp offset + rank within the warp */
 #pragma unroll
     for (int r = 0; r < E; ++r) {
@@ -721,6 +767,7 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
       if (kRadix != dig[r] && 0 == rank_w) s_wc[warp][dig[r]] += (unsigned short)__popc(peers[r]);
       __syncwarp();
     }
+    if (0 == pass) XS_CSTAMP(6);
     if (!last) { /* this pass's output is visible to the whole cluster, and s_all may be overwritten */
       cluster.sync();
 #pragma unroll
@@ -734,6 +781,8 @@ __global__ void __launch_bounds__(kClThreads) xs_stack_group_cluster_kernel(cons
       }
     }
   }
+  XS_CSTAMP(7);
+#undef XS_CSTAMP
 }
 
 /* Entries per thread kept in registers: 8 (tiles of 2048) or 16 (tiles of 4096). */
@@ -804,7 +853,7 @@ int group_launch(const xs_sort_batch_t& desc0, unsigned* k0, unsigned long long*
    cudaErrorNotSupported, launching nothing, when the device cannot run a cluster of that size. */
 int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsigned* k0, unsigned long long* v0, unsigned* k1,
   unsigned long long* v1, unsigned* kout, unsigned long long* vout, int* seglist, int* zero, int nzero, SortCtl* ctl, int ncta,
-  int heavy, cudaStream_t s) {
+  int heavy, cudaStream_t s, unsigned long long* stamps = nullptr) {
   static int ok[XS_MAXDEV][kClusterMax + 1]; /* per device and cluster size: 0 unknown, 1 supported, -1 not */
   auto kernel = xs_stack_group_cluster_kernel<kClE>;
   int* const okp = &ok[xs_device_slot()][ncta];
@@ -832,7 +881,9 @@ int cluster_group_launch(const int* stack, int S, int format, unsigned blk, unsi
     if (cudaSuccess != r) (void)cudaGetLastError(); /* not sticky: clear it */
   }
   if (0 > *okp) return (int)cudaErrorNotSupported;
-  return (int)cudaLaunchKernelEx(&cfg, kernel, stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero, ctl, heavy);
+  const unsigned blk_magic = (1u < blk) ? (unsigned)((1ull << 32) / blk) : 0u;
+  return (int)cudaLaunchKernelEx(&cfg, kernel, stack, S, format, blk, k0, v0, k1, v1, kout, vout, seglist, zero, nzero, ctl, heavy,
+    blk_magic, stamps);
 }
 
 }  // namespace
@@ -947,10 +998,11 @@ int libxstream_b200_device_error(int reset) {
   return (int)e;
 }
 
-/* Diagnostic variant: the grouping of one stack (C block size blk, 0: gcd statistics) with per-CTA
-   phase timestamps (ns, %globaltimer)
-   written to stamps[tile * 8 + phase]; allocates and frees its own buffers, synchronous. Returns the
-   number of tiles (CTAs), or a negative CUDA error code. */
+/* Diagnostic variant: the grouping of one stack (C block size blk, 0: gcd statistics) by the kernel
+   the library would use for it (one cluster up to 32768 entries, else the cooperative kernel), with
+   per-CTA phase timestamps (ns, %globaltimer) written to stamps[tile * 8 + phase]; allocates and
+   frees its own buffers, synchronous. Returns the number of tiles (CTAs), or a negative CUDA error
+   code. */
 int xs_stack_group_profile(const int* dev_stack, int S, unsigned blk, unsigned long long* host_stamps, int capacity,
   void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
@@ -963,8 +1015,12 @@ int xs_stack_group_profile(const int* dev_stack, int S, unsigned blk, unsigned l
   d.gidx[0] = 0;
   d.blk[0] = blk;
   xs_sort_batch_t dp = d;
-  int large = 0;
-  const int grid = plan_tiles(&dp, &large);
+  int large = 0, ncta = 0;
+  if (0 < S && S <= kClusterEntries) {
+    ncta = 1;
+    while (ncta * kClThreads * kClE < S) ncta <<= 1;
+  }
+  const int grid = (0 < ncta) ? ncta : plan_tiles(&dp, &large);
   if (0 == grid || capacity < grid * 8) return -(int)cudaErrorInvalidValue;
   const size_t ks = sizeof(unsigned) * (size_t)S, vs = sizeof(unsigned long long) * (size_t)S;
   char* buf = nullptr;
@@ -983,7 +1039,9 @@ int xs_stack_group_profile(const int* dev_stack, int S, unsigned blk, unsigned l
   unsigned long long* st = (unsigned long long*)p; p += 8 * sizeof(unsigned long long) * grid;
   int* seg = (int*)p; p += 256;
   p = (char*)(((uintptr_t)p + 255) & ~(uintptr_t)255);
-  int rc = group_launch(d, k0, v0, k1, v1, ko, vo, seg, p, s, st, 1);
+  int rc = (0 < ncta) ? cluster_group_launch(dev_stack, S, 0, blk, k0, v0, k1, v1, ko, vo, seg, nullptr, 0, (SortCtl*)p, ncta, 0, s, st)
+                      : cudaErrorNotSupported;
+  if (cudaErrorNotSupported == rc) rc = group_launch(d, k0, v0, k1, v1, ko, vo, seg, p, s, st, 1);
   if (0 == rc) rc = (int)cudaMemcpyAsync(host_stamps, st, 8 * sizeof(unsigned long long) * grid, cudaMemcpyDeviceToHost, s);
   cudaFreeAsync(buf, s);
   if (cudaSuccess == (cudaError_t)rc) rc = (int)cudaStreamSynchronize(s);
