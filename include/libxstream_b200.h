@@ -25,9 +25,9 @@ typedef struct libxstream_b200_stack_t {
 } libxstream_b200_stack_t;
 
 /** All stacks of one multiplication in one call: equivalent to one libsmm_acc_process per stack
-    (FP64, homogeneous, def_mnk = 1), but grouped together and run by one persistent stack kernel
-    whose CTAs take work items from all stacks, heaviest first, plus one combine kernel; the call is
-    capturable in a CUDA graph (libxstream_b200_graph_begin/end). Stacks may share pools; if two
+    (FP64, homogeneous, def_mnk = 1), but grouped together (one grouping launch for up to 16 stacks)
+    and run by one persistent stack kernel whose CTAs take work items from all stacks, heaviest
+    first, and combine C blocks that cross CTAs themselves; the call is capturable in a CUDA graph (libxstream_b200_graph_begin/end). Stacks may share pools; if two
     stacks update the same C block their contributions are added atomically (correct, but not
     bitwise reproducible). Returns -1 (nothing done) if any stack is one libsmm_acc_process would not
     handle (m*n > max_kernel_dim^2, nonpositive sizes), else 0 or a CUDA error. No counterpart in the

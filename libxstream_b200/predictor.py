@@ -260,8 +260,11 @@ def load_weights(path: Path = DEFAULT_WEIGHTS) -> np.ndarray:
 def default_config(m: int, n: int, k: int) -> int:
     """The library's default heuristic (the method without the predictor), restated: least padded
     split of ceil(dim/8) fragments into <= 4 per warp; KP = 2 when k <= 8 else 4, or the KP of the
-    shape-specialised kernel with those tiles when one exists (queried from the library)."""
+    shape-specialised kernel with those tiles when one exists (queried from the library). Removes an
+    installed predictor first (the library installs the shipped one when it initialises), since the
+    library's lookup would otherwise return the predictor's choice."""
     from . import lib as _lib
+    _lib().libxstream_b200_mlp_install(None, 0)
     out = (ctypes.c_int * 6)()
     _lib().libxstream_b200_get_params(m, n, k, 10000, out)
     return config_index(out[1], out[2], out[3])
