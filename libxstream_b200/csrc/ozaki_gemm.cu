@@ -18,19 +18,24 @@
  * Device layout: digit planes dA[s][M][Kp] and dB[s][N][Kp] (int8, K contiguous, Kp = K rounded
  * up to 16, zero padded), exponents ea[M], eb[N] (int32).
  *
- * GEMM kernel: one CTA per 128 x 128 tile of C, 6 warps. Warp 0 (one lane) streams (pair, k-block)
- * tiles of both operands into a 6-stage shared-memory ring with TMA (3-D tensor maps over the digit
- * planes, 128-byte swizzle, out-of-range rows and k read as zero); warp 1 owns all 512 tensor-memory
- * columns -- two 128 x 128 int32 accumulators and the tile's FP64 partial sum (two 32-bit columns per
- * C column) -- and one lane issues tcgen05.mma (M=128, N=128, K=32) per 32-byte K step, committing
- * each stage back to the producer and each finished diagonal to the epilogue; warps 2-5 (one
- * tensor-memory lane quarter each) read a finished accumulator with tcgen05.ld, scale it and add it
- * in FP64 to the partial sum, which stays in tensor memory from diagonal to diagonal (tcgen05.st):
- * C is read once (beta) at the first diagonal and written once at the last, instead of a
- * read-modify-write of C per diagonal. The accumulator goes back to the MMA issuer after each
- * diagonal, so the tensor cores work on diagonal d+1 while diagonal d is being recombined. Every
- * mbarrier wait is bounded: a stalled pipeline ends the kernel with an error status (per-call abort
- * word and the library's device error word) instead of a hang, leaving C unwritten.
+ * GEMM kernel, two forms (GemmForm): one CTA per 128 x BN tile of C, 6 warps. Warp 0 (one lane)
+ * streams (pair, k-block) tiles of both operands into a shared-memory ring with TMA (3-D tensor maps
+ * over the digit planes, 128-byte swizzle, out-of-range rows and k read as zero); warp 1 owns all 512
+ * tensor-memory columns and one lane issues tcgen05.mma (M=128, N=BN, K=32) per 32-byte K step,
+ * committing each stage back to the producer and each finished diagonal to the epilogue; warps 2-5
+ * (one tensor-memory lane quarter each) read a finished int32 accumulator with tcgen05.ld, scale it
+ * and add it in FP64, then hand it back, so the tensor cores work on diagonal d+1 while diagonal d is
+ * being recombined.
+ *  - partial form (BN = 128, 6 stages; M*N up to 4096^2): two 128-column accumulators and the tile's
+ *    FP64 partial sum (two 32-bit columns per C column) share tensor memory; the partial sum stays
+ *    there from diagonal to diagonal (tcgen05.st), so C is read once (beta) at the first diagonal and
+ *    written once at the last;
+ *  - read-modify-write form (BN = 256, 4 stages; larger products): two 256-column accumulators, each
+ *    diagonal added into C. A 256-wide tile needs 25 % fewer operand bytes per MAC; above 4096^2 that
+ *    outweighs the per-diagonal C traffic (measured; neither a CTA pair sharing B tiles nor shorter
+ *    K ranges per launch were faster).
+ * Every mbarrier wait is bounded: a stalled pipeline ends the kernel with an error status (per-call
+ * abort word and the library's device error word) instead of a hang.
  */
 #include "internal.h"
 #include "tc_ptx.cuh"
@@ -46,13 +51,26 @@ namespace {
 using namespace xs_tc;
 using namespace xs_oz;
 
-constexpr int kBM = 128, kBN = 128, kBK = 128, kStages = 6;
-constexpr uint32_t kPartCol = 2 * kBN; /* tensor-memory column of the FP64 partial sum (2 columns per C column) */
+/* Two forms of the GEMM kernel (GemmForm): 128 x 128 C tiles whose FP64 partial sum stays in tensor
+   memory across anti-diagonals (C read and written once; 6 stages), and 128 x 256 tiles that add each
+   diagonal into C (read-modify-write per diagonal; 4 stages, 25 % fewer operand bytes per MAC). The
+   first is faster up to M*N = 4096^2, the second above (measured on B200). */
+constexpr int kBM = 128, kBK = 128;
+template <bool PARTIAL>
+struct GemmForm {
+  static constexpr int BN = PARTIAL ? 128 : 256, STAGES = PARTIAL ? 6 : 4;
+  static constexpr int ATILE = kBM * kBK, BTILE = BN * kBK;
+  static constexpr uint32_t PART_COL = 2 * BN; /* tensor-memory column of the FP64 partial sum (2 per C column) */
+  static constexpr size_t smem_bytes() {
+    return 1024 /* alignment slack */ + (size_t)STAGES * (ATILE + BTILE) + (2 * STAGES + 4) * sizeof(uint64_t) +
+           16 /* tensor-memory address */ + BN * sizeof(int);
+  }
+};
+constexpr long long kPartialMaxMN = 4096ll * 4096ll; /* largest M*N run by the tensor-memory partial form */
 constexpr int kMaxSlices = 8;
 constexpr int kMaxPairs = kMaxSlices * kMaxSlices;
 constexpr int kMaxGroups = 2 * kMaxSlices - 1;
 constexpr int kKChunkBlocks = 16384 / kBK; /* k-blocks per launch: keeps every diagonal's int32 sum exact */
-constexpr int kATileBytes = kBM * kBK, kBTileBytes = kBN * kBK;
 constexpr int kGemmThreads = 192;
 constexpr int kGroupM = 8; /* row panels per rasterization group */
 constexpr unsigned kErrOzakiTimeout = 4u; /* device error word bit: an Ozaki pipeline wait timed out */
@@ -176,14 +194,13 @@ __device__ __forceinline__ double add_scaled(double c, int v, int E, double alph
   return fma(alpha, t, c);
 }
 
-constexpr size_t gemm_smem_bytes() {
-  return 1024 /* alignment slack */ + (size_t)kStages * (kATileBytes + kBTileBytes) + 16 * sizeof(uint64_t) + 16 +
-         kBN * sizeof(int);
-}
-
+template <bool PARTIAL>
 __global__ void __launch_bounds__(kGemmThreads, 1)
   xs_ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
     const __grid_constant__ OzGemmArgs args) {
+  using F = GemmForm<PARTIAL>;
+  constexpr int kBN = F::BN, kStages = F::STAGES, kATileBytes = F::ATILE, kBTileBytes = F::BTILE;
+  constexpr uint32_t kPartCol = F::PART_COL;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* const smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* const sA = smem;
@@ -193,7 +210,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   uint64_t* const empty = bars + kStages;
   uint64_t* const accf = bars + 2 * kStages;
   uint64_t* const acce = accf + 2;
-  uint32_t* const tmem_slot = (uint32_t*)(bars + 16);
+  uint32_t* const tmem_slot = (uint32_t*)(acce + 2);
   int* const s_eb = (int*)(tmem_slot + 4);
   unsigned* const abort = args.abort;
 
@@ -280,8 +297,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       }
     }
   }
-  else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; this lane's row of the tile keeps
-            its FP64 partial sum in tensor memory from one diagonal to the next */
+  else if constexpr (PARTIAL) { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; this lane's row
+                                   of the tile keeps its FP64 partial sum in tensor memory across diagonals */
     const int q = warp & 3;
     const int row = m0 + q * 32 + lane;
     const bool rok = row < args.M;
@@ -337,6 +354,47 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         }
       }
       if (!last_g) tmem_st_wait(); /* the partial sums are in tensor memory before the next diagonal reads them */
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+    }
+  }
+  else { /* epilogue: warps 2..5, tensor-memory lane quarter warp % 4; each diagonal is added into C */
+    const int q = warp & 3;
+    const int row = m0 + q * 32 + lane;
+    const bool rok = row < args.M;
+    const int ear = rok ? args.ea[row] : 0;
+    const uint32_t tlane = tmem + ((uint32_t)(q * 32) << 16);
+    for (int g = 0; g < args.ngroups; ++g) {
+      const int buf = g & 1, use = g >> 1;
+      if (!mbar_wait(&accf[buf], (uint32_t)use & 1u, abort, 8u, args.wait_limit)) break;
+      tc_fence_after();
+      const int eshift = args.g[g].eshift;
+      const bool beta_now = (0 != args.first) && (0 == g);
+      for (int c0 = 0; c0 < kBN; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tlane + (uint32_t)(buf * kBN + c0), v);
+        tmem_ld_wait();
+        if (rok) { /* all 32 loads of the chunk first, then the updates and the stores (no load waits for a
+                      store it cannot be proven independent of) */
+          double* const crow = args.C + row + (long long)(n0 + c0) * args.ldc;
+          const int ncol = min(32, args.N - (n0 + c0));
+          const bool read_c = !beta_now || 0.0 != args.beta;
+          double cv[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) cv[j] = (j < ncol && read_c) ? crow[(long long)j * args.ldc] : 0.0;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            double c = beta_now ? args.beta * cv[j] : cv[j];
+            const int iv = (int)v[j];
+            if (0 != iv) c = add_scaled(c, iv, ear + s_eb[c0 + j] + eshift, args.alpha);
+            cv[j] = c;
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            if (j < ncol) crow[(long long)j * args.ldc] = cv[j];
+          }
+        }
+      }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
     }
@@ -449,7 +507,8 @@ int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, c
   xs_profile_end(prof, "ozaki_slice", 0.0, 8.0 * ((double)M * K + (double)K * N), stream);
   CUtensorMap mapA, mapB;
   if (0 != (r = make_plane_map(&mapA, dA, Kp, M, nslices, kBM))) return r;
-  if (0 != (r = make_plane_map(&mapB, dB, Kp, N, nslices, kBN))) return r;
+  const bool partial = (long long)M * N <= kPartialMaxMN;
+  if (0 != (r = make_plane_map(&mapB, dB, Kp, N, nslices, partial ? GemmForm<true>::BN : GemmForm<false>::BN))) return r;
   OzGemmArgs args;
   memset(&args, 0, sizeof(args));
   args.M = M;
@@ -482,16 +541,18 @@ int xs_ozaki_gemm(char transa, char transb, int M, int N, int K, double alpha, c
     }
   }
   args.ngroups = ng;
-  const size_t smem = gemm_smem_bytes();
-  if (0 != (r = xs_func_smem((const void*)xs_ozaki_gemm_kernel, smem))) return r;
-  const int nkb = (K + kBK - 1) / kBK;
-  const dim3 grid(((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM));
+  const size_t smem = partial ? GemmForm<true>::smem_bytes() : GemmForm<false>::smem_bytes();
+  void (*const kernel)(const CUtensorMap, const CUtensorMap, const OzGemmArgs) =
+    partial ? xs_ozaki_gemm_kernel<true> : xs_ozaki_gemm_kernel<false>;
+  if (0 != (r = xs_func_smem((const void*)kernel, smem))) return r;
+  const int nkb = (K + kBK - 1) / kBK, bn = partial ? GemmForm<true>::BN : GemmForm<false>::BN;
+  const dim3 grid(((N + bn - 1) / bn) * ((M + kBM - 1) / kBM));
   for (int kb0 = 0; kb0 < nkb; kb0 += kKChunkBlocks) {
     args.kb0 = kb0;
     args.kb1 = (kb0 + kKChunkBlocks < nkb) ? kb0 + kKChunkBlocks : nkb;
     args.first = (0 == kb0) ? 1 : 0;
     prof = xs_profile_begin(stream);
-    xs_ozaki_gemm_kernel<<<grid, kGemmThreads, smem, s>>>(mapA, mapB, args);
+    kernel<<<grid, kGemmThreads, smem, s>>>(mapA, mapB, args);
     if (0 != (r = (int)cudaGetLastError())) return r;
     const double kc = (double)(args.kb1 - args.kb0) * kBK;
     xs_profile_end(prof, "ozaki_gemm", 2.0 * M * N * (kc < K ? kc : K), 0.0, stream);

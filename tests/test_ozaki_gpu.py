@@ -132,3 +132,19 @@ def test_plain_dgemm_matches_fp64(acc, shape):
     assert relerr(got, 0.5 * (a @ b) - 2.0 * c0) <= 1e-14
     for buf in (da, db, dc):
         buf.free()
+
+
+@pytest.mark.parametrize("shape,trans", [((4160, 4100, 200), "NN"), ((4097, 4200, 96), "TN")])
+def test_read_modify_write_form_above_4096_squared(acc, shape, trans):
+    """Products with M*N above 4096^2 run the 128 x 256 read-modify-write kernel form (the smaller ones
+    keep the FP64 partial sum in tensor memory): its result against numpy/BLAS FP64 with alpha, beta
+    and a ragged last tile in both directions."""
+    A, stream = acc
+    M, N, K = shape
+    g = W.rng(77 + M)
+    a_op = g.uniform(-1, 1, size=(M, K))
+    b = g.uniform(-1, 1, size=(K, N))
+    c0 = g.uniform(-1, 1, size=(M, N))
+    a = a_op if "N" == trans[0] else np.asfortranarray(a_op.T)
+    got = run(A, stream, trans[0], trans[1], M, N, K, a, b, c0, alpha=0.75, beta=-0.5, nslices=7, trim=6)
+    assert relerr(got, 0.75 * (a_op @ b) - 0.5 * c0) <= 1e-13
