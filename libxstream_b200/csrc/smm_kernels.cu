@@ -161,8 +161,8 @@ struct StackTask {
   int npf;        /* records whose A and B blocks are prefetched into L2 (0: none) */
 };
 
-/* Bulk prefetch into L2 of the A and B blocks of the first tk.npf parameter records, spread over the
-   grid's threads. It reads only the caller's inputs (the raw stack and the pools), so a stack kernel
+/* Bulk prefetch into L2 of the A and B blocks of the first tk.npf parameter records, dealt round-robin
+   over the CTAs (record i to CTA i mod grid), so that every SM's copy unit issues a share. It reads only the caller's inputs (the raw stack and the pools), so a stack kernel
    runs it before pdl_wait, while the grouping that precedes it in the stream still runs and the
    pools would otherwise be fetched only at the first copy. A block's window is widened to 16-byte
    boundaries (the bulk-copy granule); a widened window never leaves the block's page. */
@@ -174,7 +174,7 @@ __device__ __forceinline__ void prefetch_operands(const StackTask& tk) {
   if (0 >= tk.npf) return;
   const uint32_t abytes = (uint32_t)(tk.m * tk.k * sizeof(double)), bbytes = (uint32_t)(tk.k * tk.n * sizeof(double));
   const int nthreads = (int)(gridDim.x * blockDim.x);
-  for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < tk.npf; i += nthreads) {
+  for (int i = (int)(blockIdx.x + gridDim.x * threadIdx.x); i < tk.npf; i += nthreads) {
     const int* const e = tk.raw + (size_t)tk.rstride * i + tk.rbase;
     prefetch_block(tk.a + (e[0] + tk.rshift), abytes);
     prefetch_block(tk.b + (e[1] + tk.rshift), bbytes);
