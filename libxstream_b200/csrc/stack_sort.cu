@@ -350,8 +350,8 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     }
     /* (a) tile histogram, row hist[tile][0..R); per-warp counters zeroed for (c) */
     for (int d = threadIdx.x; d < R; d += blockDim.x) s_base[d] = 0;
-    for (int j = threadIdx.x; j < kSortWarps * kRadix; j += blockDim.x) {
-      if ((j & (kRadix - 1)) < R) (&s_wc[0][0])[j] = 0;
+    for (int j = threadIdx.x; j < kSortWarps * (kRadix / 8); j += blockDim.x) { /* 8 counters per 16-byte store */
+      if (8 * (j & (kRadix / 8 - 1)) < R) reinterpret_cast<uint4*>(&s_wc[0][0])[j] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
     { /* one shared-memory add per distinct digit of a warp round (hot C blocks) */
