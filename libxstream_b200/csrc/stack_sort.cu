@@ -363,7 +363,13 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
       }
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < R; d += blockDim.x) hist[(size_t)tile * kRadix + d] = s_base[d];
+    if (direct) { /* 16-bit counts (a tile holds at most kTileLarge entries): half the bytes to read in (b) */
+      unsigned short* const row16 = reinterpret_cast<unsigned short*>(hist) + (size_t)tile * kRadix;
+      for (int d = threadIdx.x; d < R; d += blockDim.x) row16[d] = (unsigned short)s_base[d];
+    }
+    else {
+      for (int d = threadIdx.x; d < R; d += blockDim.x) hist[(size_t)tile * kRadix + d] = s_base[d];
+    }
     if (0 == pass) XS_STAMP(3);
     if (!grid_sync(ctl, epoch)) return;
     if (0 == pass) XS_STAMP(4);
@@ -375,34 +381,43 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
     int tot[PER], pre[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) tot[j] = pre[j] = 0;
-    if (direct) { /* coalesced: thread t sums digits t, t + 256, ... over the stack's rows; the sums move
-                     through shared memory to the contiguous ownership the scan below uses */
+    if (direct) { /* coalesced: thread t sums the digit pairs (2q, 2q + 1), q = t, t + 256, ..., of the stack's
+                     16-bit rows, eight rows per round of loads; the sums move through shared memory to
+                     the contiguous ownership the scan below uses */
+      static_assert(0 == PER % 2, "digit pairs");
       int ctot[PER], cpre[PER];
 #pragma unroll
       for (int j = 0; j < PER; ++j) ctot[j] = cpre[j] = 0;
       if (active) {
-        for (int tt = 0; tt < G; tt += 4) {
-          int h[4][PER];
+        const unsigned short* const rows16 = reinterpret_cast<const unsigned short*>(hist) + (size_t)tb * kRadix;
+        for (int tt = 0; tt < G; tt += 8) {
+          unsigned h[8][PER / 2];
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-              const int d = j * kSortThreads + (int)threadIdx.x;
-              h[u][j] = (tt + u < G && d < R) ? __ldcg(hist + (size_t)(tb + tt + u) * kRadix + d) : 0;
+            for (int j2 = 0; j2 < PER / 2; ++j2) {
+              const int q = j2 * kSortThreads + (int)threadIdx.x;
+              h[u][j2] = (tt + u < G && 2 * q < R)
+                           ? __ldcg(reinterpret_cast<const unsigned*>(rows16 + (size_t)(tt + u) * kRadix) + q) : 0u;
             }
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-              ctot[j] += h[u][j];
-              cpre[j] += (tt + u < lt) ? h[u][j] : 0;
+            for (int j2 = 0; j2 < PER / 2; ++j2) {
+              const int lo = (int)(h[u][j2] & 0xFFFFu), hi = (2 * (j2 * kSortThreads + (int)threadIdx.x) + 1 < R) ? (int)(h[u][j2] >> 16) : 0;
+              ctot[2 * j2] += lo;
+              ctot[2 * j2 + 1] += hi;
+              if (tt + u < lt) {
+                cpre[2 * j2] += lo;
+                cpre[2 * j2 + 1] += hi;
+              }
             }
         }
       }
       int* const s_pre = reinterpret_cast<int*>(&s_wc[0][0]); /* the per-warp counters are zero and unused until (c) */
 #pragma unroll
       for (int j = 0; j < PER; ++j) {
-        const int d = j * kSortThreads + (int)threadIdx.x;
+        const int d = 2 * ((j / 2) * kSortThreads + (int)threadIdx.x) + (j & 1);
         if (d < R) {
           s_base[d] = ctot[j];
           s_pre[d] = cpre[j];
