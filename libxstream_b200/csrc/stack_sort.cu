@@ -354,13 +354,10 @@ __global__ void __launch_bounds__(kSortThreads) xs_stack_group_kernel(xs_sort_ba
       if (8 * (j & (kRadix / 8 - 1)) < R) reinterpret_cast<uint4*>(&s_wc[0][0])[j] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
-    { /* one shared-memory add per distinct digit of a warp round (hot C blocks) */
-      unsigned pr[E];
-      match_digits<E>(dig, rb, pr);
 #pragma unroll
-      for (int r = 0; r < E; ++r) {
-        if (kRadix != dig[r] && 0 == __popc(pr[r] & ((1u << lane) - 1u))) atomicAdd(&s_base[dig[r]], __popc(pr[r]));
-      }
+    for (int r = 0; r < E; ++r) { /* shared-memory atomics: lanes of a hot C block serialise on one counter,
+                                     which costs less than matching the digits first */
+      if (kRadix != dig[r]) atomicAdd(&s_base[dig[r]], 1);
     }
     __syncthreads();
     if (direct) { /* 16-bit counts (a tile holds at most kTileLarge entries): half the bytes to read in (b) */
