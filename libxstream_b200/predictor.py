@@ -8,7 +8,7 @@ and size. A sweep over many shapes is the predictor's training set: every (shape
 size) becomes samples for the exponent spreads {0, 10, 40} with targets r_c = t_c / t_best and the
 Ozaki label (Ozaki faster than the best plain configuration). The network (3 x FP32 width 64, see
 csrc/mlp.cu) is trained on the device by the library's own kernels; the exhaustive tuner is its
-fallback (shapes where the network is not confident are tuned) and its judge (held-out shapes are
+fallback (shapes where the network is not confident are tuned) and its referee (held-out shapes are
 scored by the measured time of the predicted configuration against the tuned optimum).
 
 Command line (one GPU):
