@@ -144,3 +144,19 @@ def test_near_cancellation(acc):
     ref = O.ozaki2_gemm(a, b, O.default_moduli(K))
     assert np.max(np.abs(ref)) < 1e-4
     assert relerr(got, ref) <= RECON_TOL
+
+
+def test_benchmark_size_against_numpy(acc):
+    """N = 4096, the smallest square of the GEMM benchmark above 2048, uniform and row-scaled (2^u,
+    u in [-30, 30]) inputs, against numpy/BLAS FP64 (an oracle independent of the library's DMMA GEMM)."""
+    A, stream = acc
+    N = 4096
+    g = W.rng(4096)
+    a = g.uniform(-1, 1, size=(N, N))
+    b = g.uniform(-1, 1, size=(N, N))
+    got = run(A, stream, "N", "N", N, N, N, a, b, np.zeros((N, N)))
+    assert relerr(got, a @ b) <= FP64_TOL
+    a_rs = a * np.exp2(g.integers(-30, 31, size=N))[:, None]
+    got = run(A, stream, "N", "N", N, N, N, a_rs, b, np.zeros((N, N)))
+    ref = a_rs @ b
+    assert float(np.max(np.max(np.abs(got - ref), axis=1) / np.max(np.abs(ref), axis=1))) <= FP64_TOL

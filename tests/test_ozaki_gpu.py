@@ -148,3 +148,16 @@ def test_read_modify_write_form_above_4096_squared(acc, shape, trans):
     a = a_op if "N" == trans[0] else np.asfortranarray(a_op.T)
     got = run(A, stream, trans[0], trans[1], M, N, K, a, b, c0, alpha=0.75, beta=-0.5, nslices=7, trim=6)
     assert relerr(got, 0.75 * (a_op @ b) - 0.5 * c0) <= 1e-13
+
+
+@pytest.mark.parametrize("N", [4096, 4104])
+def test_benchmark_size_against_numpy(acc, N):
+    """Square sizes of the GEMM benchmark, s = 7 triangle, against numpy/BLAS FP64 (an oracle independent
+    of the library's DMMA GEMM): 4096 runs the tensor-memory partial form, 4104 (just above 4096^2)
+    the read-modify-write form."""
+    A, stream = acc
+    g = W.rng(N)
+    a = g.uniform(-1, 1, size=(N, N))
+    b = g.uniform(-1, 1, size=(N, N))
+    got = run(A, stream, "N", "N", N, N, N, a, b, np.zeros((N, N)), beta=0.0, nslices=7, trim=6)
+    assert relerr(got, a @ b) <= 1e-13
