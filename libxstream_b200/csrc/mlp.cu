@@ -219,17 +219,67 @@ __global__ void xs_mlp_adam(float* __restrict__ W, const float* __restrict__ G, 
   W[w] -= lr * mh / (sqrtf(vh) + eps);
 }
 
-/* Inference, after xs_mlp_fwd: masked argmax over the configurations, its softmax probability and
-   the Ozaki probability. */
-__global__ void xs_mlp_select(const float* __restrict__ Y, const int* __restrict__ raw, const unsigned char* __restrict__ fma_ok,
-  int N, unsigned char* __restrict__ cfg, float* __restrict__ conf, float* __restrict__ pz) {
+/* Inference only: features, forward pass and selection per sample with the activations in registers
+   (layer by layer over the inputs, four or two weights per shared-memory load), writing nothing but
+   the selected configuration, its probability and the Ozaki probability. The same fmaf sequence per
+   output as forward_one, so the logits are bitwise those of xs_mlp_fwd. */
+__global__ void __launch_bounds__(128) xs_mlp_infer(const float* __restrict__ W, const int* __restrict__ raw,
+  const unsigned char* __restrict__ fma_ok, int N, unsigned char* __restrict__ cfg, float* __restrict__ conf,
+  float* __restrict__ pz) {
+  extern __shared__ __align__(16) float sW[];
+  load_weights(W, sW);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const float* y = Y + (size_t)i * O;
+  static_assert(0 == (oW1 % 4) && 0 == (oW2 % 4) && 0 == (H % 4) && 0 == (oW3 % 2) && 0 == (O % 2), "vector weight loads");
+  float x[F];
+  features(raw + 5 * (size_t)i, x);
+  float h1[H], h2[H], y[O];
+#pragma unroll
+  for (int h = 0; h < H; ++h) h1[h] = sW[ob1 + h];
+#pragma unroll
+  for (int f = 0; f < F; ++f) {
+#pragma unroll
+    for (int h = 0; h < H; h += 4) {
+      const float4 w = *reinterpret_cast<const float4*>(sW + oW1 + f * H + h);
+      h1[h] = fmaf(x[f], w.x, h1[h]);
+      h1[h + 1] = fmaf(x[f], w.y, h1[h + 1]);
+      h1[h + 2] = fmaf(x[f], w.z, h1[h + 2]);
+      h1[h + 3] = fmaf(x[f], w.w, h1[h + 3]);
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < H; ++h) h1[h] = fmaxf(h1[h], 0.f);
+#pragma unroll
+  for (int j = 0; j < H; ++j) h2[j] = sW[ob2 + j];
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+#pragma unroll
+    for (int j = 0; j < H; j += 4) {
+      const float4 w = *reinterpret_cast<const float4*>(sW + oW2 + h * H + j);
+      h2[j] = fmaf(h1[h], w.x, h2[j]);
+      h2[j + 1] = fmaf(h1[h], w.y, h2[j + 1]);
+      h2[j + 2] = fmaf(h1[h], w.z, h2[j + 2]);
+      h2[j + 3] = fmaf(h1[h], w.w, h2[j + 3]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < H; ++j) h2[j] = fmaxf(h2[j], 0.f);
+#pragma unroll
+  for (int o = 0; o < O; ++o) y[o] = sW[ob3 + o];
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+#pragma unroll
+    for (int o = 0; o < O; o += 2) {
+      const float2 w = *reinterpret_cast<const float2*>(sW + oW3 + j * O + o);
+      y[o] = fmaf(h2[j], w.x, y[o]);
+      y[o + 1] = fmaf(h2[j], w.y, y[o + 1]);
+    }
+  }
   const int m = raw[5 * (size_t)i], n = raw[5 * (size_t)i + 1];
   const bool fok = (nullptr != fma_ok) && 0 != fma_ok[i];
   int best = 0;
   float ymax = -INFINITY;
+#pragma unroll
   for (int c = 0; c < K; ++c) {
     if (config_valid(c, m, n, fok) && y[c] > ymax) {
       ymax = y[c];
@@ -237,12 +287,13 @@ __global__ void xs_mlp_select(const float* __restrict__ Y, const int* __restrict
     }
   }
   float z = 0.f;
+#pragma unroll
   for (int c = 0; c < K; ++c) {
     if (config_valid(c, m, n, fok)) z += expf(y[c] - ymax);
   }
   cfg[i] = (unsigned char)best;
-  conf[i] = 1.f / z;
-  pz[i] = 1.f / (1.f + expf(-y[K]));
+  if (nullptr != conf) conf[i] = 1.f / z;
+  if (nullptr != pz) pz[i] = 1.f / (1.f + expf(-y[K]));
 }
 
 struct Dev {
@@ -297,7 +348,8 @@ int grad_pass(Dev& d, int N, cudaStream_t s) {
 
 int set_smem_attrs(void) {
   const size_t smem = sizeof(float) * NW;
-  const int r = xs_func_smem((const void*)xs_mlp_fwd, smem);
+  int r = xs_func_smem((const void*)xs_mlp_fwd, smem);
+  if (0 == r) r = xs_func_smem((const void*)xs_mlp_infer, smem);
   return (0 != r) ? r : xs_func_smem((const void*)xs_mlp_bwd, smem);
 }
 
@@ -389,13 +441,14 @@ int xs_mlp_forward(const float* weights, const int* raw, int N, float* y) {
 }
 
 /* Inference for N queries (m, n, k, S, spread): configuration index, its probability, Ozaki
-   probability. Synchronous. */
+   probability (conf, pz may be null). Synchronous. Device memory: the weights and about 30 bytes per
+   query (queries, FMA flags and the three results); the training buffers are not touched. */
 int xs_mlp_predict(const float* weights, const int* raw, int N, unsigned char* cfg, float* conf, float* pz) {
-  Dev d;
   if (N < 1) return 0;
   int r = set_smem_attrs();
   if (0 != r) return r;
-  if (0 != (r = dev_alloc(d, N))) return r;
+  float *dW = nullptr, *dconf = nullptr, *dpz = nullptr;
+  int* draw = nullptr;
   unsigned char *dcfg = nullptr, *dfma = nullptr;
   /* where the FMA kernel takes the shape (host-side rule, the same one its launcher applies) */
   unsigned char* const fma_ok = (unsigned char*)malloc((size_t)N);
@@ -403,23 +456,29 @@ int xs_mlp_predict(const float* weights, const int* raw, int N, unsigned char* c
   else {
     for (int i = 0; i < N; ++i) fma_ok[i] = (unsigned char)xs_smm_fma_supported(raw[5 * (size_t)i], raw[5 * (size_t)i + 1], raw[5 * (size_t)i + 2]);
   }
+  if (0 == r) r = (int)cudaMalloc(&dW, sizeof(float) * NW);
+  if (0 == r) r = (int)cudaMalloc(&draw, sizeof(int) * 5 * (size_t)N);
   if (0 == r) r = (int)cudaMalloc(&dcfg, (size_t)N);
   if (0 == r) r = (int)cudaMalloc(&dfma, (size_t)N);
+  if (0 == r) r = (int)cudaMalloc(&dconf, sizeof(float) * (size_t)N);
+  if (0 == r) r = (int)cudaMalloc(&dpz, sizeof(float) * (size_t)N);
   if (0 == r) r = (int)cudaMemcpy(dfma, fma_ok, (size_t)N, cudaMemcpyHostToDevice);
-  if (0 == r) r = (int)cudaMemcpy(d.raw, raw, sizeof(int) * 5 * (size_t)N, cudaMemcpyHostToDevice);
-  if (0 == r) r = (int)cudaMemcpy(d.W, weights, sizeof(float) * NW, cudaMemcpyHostToDevice);
+  if (0 == r) r = (int)cudaMemcpy(draw, raw, sizeof(int) * 5 * (size_t)N, cudaMemcpyHostToDevice);
+  if (0 == r) r = (int)cudaMemcpy(dW, weights, sizeof(float) * NW, cudaMemcpyHostToDevice);
   if (0 == r) {
-    xs_mlp_fwd<<<(N + 127) / 128, 128, sizeof(float) * NW>>>(d.W, d.raw, N, d.X, d.H1, d.H2, d.Y);
-    xs_mlp_select<<<(N + 127) / 128, 128>>>(d.Y, d.raw, dfma, N, dcfg, d.loss, d.Z);
+    xs_mlp_infer<<<(N + 127) / 128, 128, sizeof(float) * NW>>>(dW, draw, dfma, N, dcfg, dconf, dpz);
     r = (int)cudaGetLastError();
   }
   if (0 == r) r = (int)cudaMemcpy(cfg, dcfg, (size_t)N, cudaMemcpyDeviceToHost);
-  if (0 == r && nullptr != conf) r = (int)cudaMemcpy(conf, d.loss, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost);
-  if (0 == r && nullptr != pz) r = (int)cudaMemcpy(pz, d.Z, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost);
-  cudaFree(dcfg);
+  if (0 == r && nullptr != conf) r = (int)cudaMemcpy(conf, dconf, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost);
+  if (0 == r && nullptr != pz) r = (int)cudaMemcpy(pz, dpz, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost);
+  cudaFree(dpz);
+  cudaFree(dconf);
   cudaFree(dfma);
+  cudaFree(dcfg);
+  cudaFree(draw);
+  cudaFree(dW);
   free(fma_ok);
-  dev_free(d);
   return r;
 }
 
