@@ -159,7 +159,22 @@ struct StackTask {
   int rbase;      /* a-offset position within a record (b follows) */
   int rshift;     /* added to a record's offsets to make them 0-based (-1: 1-based, 0: 0-based) */
   int npf;        /* records whose A and B blocks are prefetched into L2 (0: none) */
+  int Ls[3];      /* entries per chunk in the CTA groups [0, slotn), [slotn, 2 slotn), [2 slotn, ...) */
+  int slotn;      /* CTA groups per length class (the SM count when the lengths differ) */
 };
+
+/* First entry of chunk c (0 <= c <= nchunks; S at the end) when CTA group b = c / W holds W chunks
+   of Ls[class of b] entries. The host makes the three lengths equal (chunk c starts at c L), or, for
+   a one-wave launch of several CTAs per SM, longer for the CTAs launched first on their SM and
+   shorter for the last ones: the SM's warp schedulers favour its older CTAs, so equal chunks leave
+   the last-launched CTA's warps running alone at the end. */
+__device__ __forceinline__ int chunk_first(const StackTask& tk, int W, int c) {
+  const int b = c / W, w = c - b * W, sn = tk.slotn;
+  const long long n0 = min(b, sn), n1 = min(max(b - sn, 0), sn), n2 = max(b - 2 * sn, 0);
+  const int Lb = (b < sn) ? tk.Ls[0] : ((b < 2 * sn) ? tk.Ls[1] : tk.Ls[2]);
+  const long long f = (long long)W * (n0 * tk.Ls[0] + n1 * tk.Ls[1] + n2 * tk.Ls[2]) + (long long)w * Lb;
+  return (int)min(f, (long long)tk.S);
+}
 
 /* Bulk prefetch into L2 of the A and B blocks of the first tk.npf parameter records, dealt round-robin
    over the CTAs (record i to CTA i mod grid), so that every SM's copy unit issues a share. It reads only the caller's inputs (the raw stack and the pools), so a stack kernel
@@ -208,19 +223,19 @@ constexpr int kFan = 8;
 __device__ __forceinline__ int piece_slot(int j0, int q) { return (0 == q) ? 2 * j0 + 1 : 2 * (j0 + q); }
 
 /* Groups j0 <= j <= j1 (j0, j1 returned) that hold entries of the segment with key x, for a segment
-   that the CTA group j (W chunks of L entries, Lc = W*L) holds and that crosses j's first boundary
-   (head: entry j*Lc - 1 has key x)
-   and/or its last one (tail: entry (j+1)*Lc has key x). Keys are sorted, so the boundaries a segment
+   that the CTA group j (W chunks, chunk_first) holds and that crosses j's first boundary (head: the
+   entry before the group's first one has key x) and/or its last one (tail: the first entry of group
+   j + 1 has key x). Keys are sorted, so the boundaries a segment
    crosses are consecutive: one warp tests 32 boundaries per round (one load per lane). */
 __device__ __forceinline__ void segment_groups(const StackTask& tk, int W, int j, unsigned x, bool head, bool tail, int& j0,
   int& j1) {
-  const int lane = threadIdx.x & 31, Lc = tk.L * W;
+  const int lane = threadIdx.x & 31;
   const unsigned* __restrict__ const keys = tk.keys;
   j0 = j;
-  if (head) { /* boundary j - q (start of group j - q) is crossed iff entry (j - q) * Lc - 1 has key x */
+  if (head) { /* boundary j - q is crossed iff the entry before group j - q's first one has key x */
     for (int q0 = 1;; q0 += 32) {
       const int gq = j - q0 - lane;
-      const bool crossed = (gq >= 1) && __ldcg(keys + (size_t)gq * Lc - 1) == x;
+      const bool crossed = (gq >= 1) && __ldcg(keys + (size_t)chunk_first(tk, W, gq * W) - 1) == x;
       const unsigned m = __ballot_sync(0xFFFFFFFFu, crossed);
       if (0xFFFFFFFFu != m) {
         j0 = j - q0 - (__ffs(~m) - 1);
@@ -232,7 +247,7 @@ __device__ __forceinline__ void segment_groups(const StackTask& tk, int W, int j
   if (tail) { /* group j + 1 holds x; group j + q (q >= 2) does iff its first entry has key x */
     for (int q0 = 2;; q0 += 32) {
       const int gq = j + q0 + lane;
-      const bool crossed = (gq < tk.ngroups) && __ldcg(keys + (size_t)gq * Lc) == x;
+      const bool crossed = (gq < tk.ngroups) && __ldcg(keys + (size_t)chunk_first(tk, W, gq * W)) == x;
       const unsigned m = __ballot_sync(0xFFFFFFFFu, crossed);
       if (0xFFFFFFFFu != m) {
         j1 = j + q0 - 1 + (__ffs(~m) - 1);
@@ -248,7 +263,7 @@ __device__ __forceinline__ void segment_groups(const StackTask& tk, int W, int j
    one warp computes them while the CTA's first copies are in flight, and the merge at the end does
    not wait for these loads. Called by a whole warp; lane 0 writes probe. */
 __device__ __forceinline__ void probe_boundaries(const StackTask& tk, int W, int group, int* probe) {
-  const int S = tk.S, first = group * tk.L * W, lastp = min(first + tk.L * W, S) - 1;
+  const int S = tk.S, first = chunk_first(tk, W, group * W), lastp = chunk_first(tk, W, (group + 1) * W) - 1;
   const unsigned* __restrict__ const keys = tk.keys;
   const unsigned k0 = keys[first], k1 = keys[lastp];
   const bool hx = (0 < first) && keys[first - 1] == k0;
@@ -306,7 +321,7 @@ __device__ __forceinline__ void cta_merge(const StackTask& tk, int group, int su
     }
     const int c_first = group * W + warp; /* chunk where this chain starts */
     /* the chain's segment: the CTA's first key (head chain) or the last key of its first chunk */
-    const unsigned key = from_head ? tk.keys[(size_t)group * W * L] : tk.keys[min((c_first + 1) * L, S) - 1];
+    const unsigned key = from_head ? tk.keys[chunk_first(tk, W, group * W)] : tk.keys[chunk_first(tk, W, c_first + 1) - 1];
     if (from_head || spans) { /* the segment crosses a CTA boundary: CTA-level piece */
       const int slot = from_head ? 2 * group : 2 * group + 1;
       double* const dst = tk.pieces + ((size_t)slot * nsub + sub) * REGS * 32 + lane;
@@ -483,7 +498,7 @@ __device__ __forceinline__ void smm_item(const StackTask& tk, int group, int sub
   }
   __syncwarp();
   if (chunk < nchunks) {
-    const int p0 = chunk * L, p1 = min(p0 + L, S);
+    const int p0 = chunk_first(tk, W, chunk), p1 = chunk_first(tk, W, chunk + 1);
     const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
     const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
 
@@ -721,7 +736,7 @@ __device__ __forceinline__ bool staged_item(const StackTask& tk, int group, int*
   int head = 0, hspans = 0, tail = 0;
   bool bad = false;
   if (chunk < tk.nchunks) {
-    const int p0 = chunk * L, p1 = min(p0 + L, S);
+    const int p0 = chunk_first(tk, W, chunk), p1 = chunk_first(tk, W, chunk + 1);
     const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
     const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
     int wb = p0; /* first entry of the current window */
@@ -990,7 +1005,8 @@ __global__ void __launch_bounds__(32 * (NC + 1), MINB)
   int issued = 0; /* producer lane w: entries of chunk w whose copies were issued */
   if (NC == warp) { /* ------------------------------------------------------------- producer */
     const int chunk = group * NC + lane;
-    const int p0 = chunk * L, n = (lane < NC && chunk < tk.nchunks) ? min(L, S - p0) : 0;
+    const int p0 = (lane < NC && chunk < tk.nchunks) ? chunk_first(tk, NC, chunk) : 0;
+    const int n = (lane < NC && chunk < tk.nchunks) ? chunk_first(tk, NC, chunk + 1) - p0 : 0;
     unsigned char* const ring = smraw + (size_t)lane * G::warp_bytes(R);
     unsigned long long vnext = (0 < n) ? vals[p0] : 0ull;
     long long t_prog = clock64();
@@ -1038,7 +1054,7 @@ __global__ void __launch_bounds__(32 * (NC + 1), MINB)
       for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = hacc[i][j][0] = hacc[i][j][1] = 0.0;
     int head = 0, hspans = 0, tail = 0, consumed = 0;
     if (chunk < tk.nchunks) {
-      const int p0 = chunk * L, p1 = min(p0 + L, S);
+      const int p0 = chunk_first(tk, NC, chunk), p1 = chunk_first(tk, NC, chunk + 1);
       const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
       const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
       int wb = p0;
@@ -1287,7 +1303,7 @@ __global__ void __launch_bounds__(128, 2)
   for (int r = 0; r < REGS; ++r) acc[r] = 0.0;
   int head = 0, hspans = 0, tail = 0;
   if (chunk < tk.nchunks) {
-    const int p0 = chunk * L, p1 = min(p0 + L, S);
+    const int p0 = chunk_first(tk, W, chunk), p1 = chunk_first(tk, W, chunk + 1);
     const bool headcross = (0 < p0) && (keys[p0 - 1] == keys[p0]);
     const bool tailcross = (p1 < S) && (keys[p1 - 1] == keys[p1]);
     int wb = p0;
@@ -1467,13 +1483,13 @@ __device__ __forceinline__ void combine_one(const StackTask& tk, int W, int j0, 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const unsigned* __restrict__ const keys = tk.keys;
   const double* __restrict__ const pieces = tk.pieces;
-  const int S = tk.S, Lc = tk.L * W, ngroups = tk.ngroups, nsub = tk.nsub;
-  const unsigned xkey = keys[min((j0 + 1) * Lc, S) - 1];
+  const int ngroups = tk.ngroups, nsub = tk.nsub;
+  const unsigned xkey = keys[chunk_first(tk, W, (j0 + 1) * W) - 1];
   /* pieces = 1 + number of following groups that start inside the segment (a prefix, keys sorted) */
   int np = 1;
   for (int base = j0 + 1;; base += blockDim.x) {
     const int j = base + (int)threadIdx.x;
-    const int inside = (j < ngroups) && (keys[(size_t)j * Lc] == xkey);
+    const int inside = (j < ngroups) && (keys[(size_t)chunk_first(tk, W, j * W)] == xkey);
     const int cnt = __syncthreads_count(inside);
     np += cnt;
     if (cnt < (int)blockDim.x) break;
@@ -1659,6 +1675,7 @@ int uni_staged_index(int m, int n, int k) {
 
 struct SmmPlan {
   int nsub_m, nsub_n, nsub, nchunks, L, W, ngroups;
+  int Ls[3], slotn; /* chunk lengths per CTA length class (chunk_first) */
   int no_combine; /* the stack kernel only: CTA-crossing pieces are combined by the caller */
   size_t off_keys_in, off_keys_tmp, off_keys_out, off_vals_in, off_vals_tmp, off_vals_out, off_seglist, off_pieces;
   size_t off_arrive, off_sort, total;
@@ -1678,8 +1695,31 @@ int fma_piece_regs(int m, int n, int k);
 
 /* Work decomposition and scratch layout of one call. An open chunk length (prm->chunk <= 0) is
    sized so that the grid is one full wave of resident CTAs: L = ceil(S * nsub / (resident * W)). */
+/* Fraction of the chunk length moved from the CTA groups launched last on their SM to the ones
+   launched first (chunk_first), for one-wave launches of three CTAs per SM: 12 % (measured on B200,
+   23^3 and 22^3 stacks of 30000 entries: 6-12 % shorten the step by about 1.5 %, 18 % and more
+   lengthen it); LIBXSTREAM_B200_CHUNK_SKEW (percent, 0 = equal chunks) overrides it. */
+static double chunk_skew() {
+  static const double v = []() -> double {
+    const char* const env = getenv("LIBXSTREAM_B200_CHUNK_SKEW");
+    const double pc = (nullptr != env) ? atof(env) : 12.0;
+    return (0.0 < pc && pc < 50.0) ? pc / 100.0 : 0.0;
+  }();
+  return v;
+}
+
+/* Chunks that start before S under the plan's lengths (the host side of chunk_first). */
+static int plan_nchunks(const SmmPlan& pl, int S) {
+  if (pl.Ls[0] == pl.Ls[1] && pl.Ls[1] == pl.Ls[2]) return (S + pl.L - 1) / pl.L;
+  const long long cap0 = (long long)pl.W * pl.slotn * pl.Ls[0], cap1 = (long long)pl.W * pl.slotn * pl.Ls[1];
+  if (S <= cap0) return (int)((S + pl.Ls[0] - 1) / pl.Ls[0]);
+  if (S <= cap0 + cap1) return pl.W * pl.slotn + (int)((S - cap0 + pl.Ls[1] - 1) / pl.Ls[1]);
+  return 2 * pl.W * pl.slotn + (int)((S - cap0 - cap1 + pl.Ls[2] - 1) / pl.Ls[2]);
+}
+
 int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl) {
   const int mt = prm->mt, nt = prm->nt;
+  double auto_skew = 0.0;
   if (mt < 1 || mt > 8 || nt < 1 || nt > 8) return -1; /* tiles beyond 4 fragments: staged kernels only */
   pl->no_combine = 0;
   pl->nsub_m = ((m + 7) / 8 + mt - 1) / mt;
@@ -1702,8 +1742,20 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
     const long resident = (long)occ * xs_sm_count();
     const long L = ((long)S * pl->nsub + resident * pl->W - 1) / (resident * pl->W);
     pl->L = (int)(L < 1 ? 1 : L);
+    auto_skew = (3 == occ && 1 == pl->nsub) ? chunk_skew() : 0.0;
   }
-  pl->nchunks = (S + pl->L - 1) / pl->L;
+  pl->Ls[0] = pl->Ls[1] = pl->Ls[2] = pl->L;
+  pl->slotn = 1 << 29;
+  {
+    const int d = (int)(auto_skew * pl->L + 0.5);
+    if (0 < d && d < pl->L) { /* a one-wave launch of three CTAs per SM: the first-launched third of the
+                                 CTA groups takes L + d entries per chunk, the last third L - d */
+      pl->Ls[0] = pl->L + d;
+      pl->Ls[2] = pl->L - d;
+      pl->slotn = xs_sm_count();
+    }
+  }
+  pl->nchunks = plan_nchunks(*pl, S);
   pl->ngroups = (pl->nchunks + pl->W - 1) / pl->W;
   size_t off = 0;
   const size_t ks = align_up(sizeof(unsigned) * (size_t)S, 256), vs = align_up(sizeof(unsigned long long) * (size_t)S, 256);
@@ -2340,6 +2392,10 @@ int xs_launch_smm_f64_ex(const int* dev_stack, int S, int format, double alpha, 
   tk.nsub_n = pl.nsub_n;
   tk.nsub = pl.nsub;
   tk.arrive = arrive; /* CTA-crossing segments are combined inside the stack kernel */
+  tk.Ls[0] = pl.Ls[0];
+  tk.Ls[1] = pl.Ls[1];
+  tk.Ls[2] = pl.Ls[2];
+  tk.slotn = pl.slotn;
   set_prefetch(tk, dev_stack, S, format, prefetch_budget());
   const launch_fn_t fn = find_launcher(m, n, k, prm);
   return (int)fn(pl, tk, seglist, xs_sort_error_flag(sort_scratch), s, nullptr);
@@ -2435,6 +2491,8 @@ int xs_launch_smm_batch(const libxstream_b200_stack_t* st, int ns, void* scratch
     tk.n = d.n;
     tk.k = d.k;
     tk.L = p.L;
+    tk.Ls[0] = tk.Ls[1] = tk.Ls[2] = p.L;
+    tk.slotn = 1 << 29;
     tk.nchunks = (p.S + p.L - 1) / p.L;
     tk.ngroups = p.ngroups;
     tk.nsub_n = p.nsub_n;
