@@ -189,6 +189,8 @@ int xs_sort_launch_tiles(void);
 int xs_sort_tile_entries(int large);
 size_t xs_stack_sort_scratch_bytes(int S);
 size_t xs_stack_sort_scratch_bytes_batch(const xs_sort_batch_t* desc);
+/** Largest stack the one-cluster grouping kernel takes (entries). */
+int xs_stack_group_cluster_max(void);
 /** Largest single stack xs_stack_group takes in one launch (larger stacks are processed in parts). */
 int xs_stack_group_max(void);
 /** 1 if the batch fits one grouping launch. */

@@ -1696,9 +1696,11 @@ int fma_piece_regs(int m, int n, int k);
 /* Work decomposition and scratch layout of one call. An open chunk length (prm->chunk <= 0) is
    sized so that the grid is one full wave of resident CTAs: L = ceil(S * nsub / (resident * W)). */
 /* Fraction of the chunk length moved from the CTA groups launched last on their SM to the ones
-   launched first (chunk_first), for one-wave launches of three CTAs per SM: 12 % (measured on B200,
-   23^3 and 22^3 stacks of 30000 entries: 6-12 % shorten the step by about 1.5 %, 18 % and more
-   lengthen it); LIBXSTREAM_B200_CHUNK_SKEW (percent, 0 = equal chunks) overrides it. */
+   launched first (chunk_first), for one-wave launches of three CTAs per SM of stacks the one-cluster
+   grouping takes: 12 % (measured on B200: 23^3 and 22^3 stacks of 30000 entries 6-12 % shorten the
+   step by about 1.5 %, 18 % and more lengthen it; 32x9x9 at 10^5 entries and the shapes that run two
+   CTAs per SM were slower with it, so they keep equal chunks); LIBXSTREAM_B200_CHUNK_SKEW (percent,
+   0 = equal chunks) overrides the 12 %. */
 static double chunk_skew() {
   static const double v = []() -> double {
     const char* const env = getenv("LIBXSTREAM_B200_CHUNK_SKEW");
@@ -1742,7 +1744,7 @@ int plan_smm(int S, int m, int n, int k, const xs_smm_params_t* prm, SmmPlan* pl
     const long resident = (long)occ * xs_sm_count();
     const long L = ((long)S * pl->nsub + resident * pl->W - 1) / (resident * pl->W);
     pl->L = (int)(L < 1 ? 1 : L);
-    auto_skew = (3 == occ && 1 == pl->nsub) ? chunk_skew() : 0.0;
+    auto_skew = (3 == occ && 1 == pl->nsub && S <= xs_stack_group_cluster_max()) ? chunk_skew() : 0.0;
   }
   pl->Ls[0] = pl->Ls[1] = pl->Ls[2] = pl->L;
   pl->slotn = 1 << 29;

@@ -929,6 +929,8 @@ size_t xs_stack_sort_scratch_bytes(int S) {
   return xs_stack_sort_scratch_bytes_batch(&d);
 }
 
+int xs_stack_group_cluster_max(void) { return kClusterEntries; }
+
 int xs_stack_group_max(void) { return (sort_grid_max() < kMaxGroupTiles ? sort_grid_max() : kMaxGroupTiles) * kTileLarge; }
 
 int xs_stack_group_batch(const xs_sort_batch_t* desc, unsigned* k0, unsigned long long* v0, unsigned* k1,
